@@ -1,0 +1,11 @@
+"""gpumode_cholesky_b200 -- batched Cholesky (potrf) for NVIDIA B200 (sm_100a).
+
+Drop-in for the GPU MODE ``cholesky`` entry point ``custom_kernel(A) -> L``
+(binga/gpumode_cholesky, submission.py:4101-4268): hand-written CUDA kernels
+behind a C ABI (``include/b200_potrf.h``), called from Python through ctypes.
+"""
+
+from ._lib import PotrfError
+from .potrf import cholesky, custom_kernel
+
+__all__ = ["PotrfError", "cholesky", "custom_kernel"]

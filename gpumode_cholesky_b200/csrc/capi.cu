@@ -1,0 +1,122 @@
+// extern "C" entry points (include/b200_potrf.h) and the shape dispatcher.
+//
+// The dispatcher replaces the reference's exact-(batch, n) routing in
+// custom_kernel (submission.py:4101-4268) by routing on n alone:
+//   n <= 32    one warp per matrix            (potrf_warp32_kernel)
+//   n <= 128   one CTA per matrix, in smem    (potrf_cta128_kernel)
+//   n >  128   blocked right-looking          (potrf_blocked)
+// There is no CPU path and no vendor-library fallback.
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+
+#include "launch.h"
+
+namespace b2p {
+
+namespace {
+thread_local char g_msg[512] = "";
+constexpr int kMaxDevices = 64;
+int g_sms[kMaxDevices] = {0};
+size_t g_smem_attr[kMaxDevices][kSlotCount] = {{0}};
+std::mutex g_attr_mu;
+}  // namespace
+
+int set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return B2P_OK;
+}
+
+static int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+  return dev;
+}
+
+int device_sms() {
+  const int dev = current_device();
+  if (g_sms[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    g_sms[dev] = v;
+  }
+  return g_sms[dev];
+}
+
+int ensure_smem_attr(const void* func, size_t bytes, int slot) {
+  const int dev = current_device();
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  if (g_smem_attr[dev][slot] >= bytes) return B2P_OK;
+  const cudaError_t e =
+      cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess)
+    return set_error(B2P_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  g_smem_attr[dev][slot] = bytes;
+  return B2P_OK;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+static int check_mode(int mode) {
+  const int m = mode & B2P_MODE_MASK;
+  if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG)) != 0)
+    return set_error(B2P_ERR_INVALID_ARG, "unknown mode 0x%x", mode);
+  return B2P_OK;
+}
+
+}  // namespace b2p
+
+using namespace b2p;
+
+extern "C" {
+
+int b2p_version(void) { return 100; }
+
+const char* b2p_status_string(int status) {
+  switch (status) {
+    case B2P_OK: return "ok";
+    case B2P_ERR_INVALID_ARG: return "invalid argument";
+    case B2P_ERR_UNSUPPORTED: return "unsupported mode or size";
+    case B2P_ERR_WORKSPACE: return "workspace missing or too small";
+    case B2P_ERR_CUDA: return "CUDA error";
+    case B2P_ERR_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+  }
+}
+
+const char* b2p_last_error(void) { return g_msg; }
+
+size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode) {
+  if (batch <= 0 || n <= 128) return 0;
+  return blocked_workspace_bytes(batch, n, mode);
+}
+
+int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mode,
+                      void* workspace, size_t workspace_bytes, int32_t* info, void* stream) {
+  g_msg[0] = '\0';
+  if (int st = check_mode(mode)) return st;
+  if (batch < 0 || n < 0 || n > (1 << 20))
+    return set_error(B2P_ERR_INVALID_ARG, "bad shape batch=%lld n=%lld", (long long)batch, (long long)n);
+  if (batch == 0 || n == 0) return B2P_OK;
+  if (a == nullptr || l == nullptr) return set_error(B2P_ERR_INVALID_ARG, "null matrix pointer");
+  if (!aligned16(a) || !aligned16(l)) return set_error(B2P_ERR_INVALID_ARG, "buffers must be 16-byte aligned");
+  const size_t bytes = (size_t)batch * (size_t)n * (size_t)n * sizeof(float);
+  const char* pa = reinterpret_cast<const char*>(a);
+  const char* pl = reinterpret_cast<const char*>(l);
+  if (pa < pl + bytes && pl < pa + bytes) return set_error(B2P_ERR_INVALID_ARG, "input and output overlap");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
+  if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
+  return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+}
+
+}  // extern "C"

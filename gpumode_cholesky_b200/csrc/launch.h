@@ -1,0 +1,82 @@
+// Host-side declarations shared by the translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/b200_potrf.h"
+#include "matrix_list.cuh"
+
+namespace b2p {
+
+int set_error(int status, const char* fmt, ...);
+int check_launch(const char* what);
+
+// Multiprocessor count of the current device (cached per device).
+int device_sms();
+
+// Raises a kernel's dynamic shared-memory limit once per device.
+int ensure_smem_attr(const void* func, size_t bytes, int slot);
+
+// Whole-matrix kernels (potrf_small.cu).
+int launch_warp32(const float* a, float* l, const MatrixList& ml, int32_t* info, cudaStream_t s);
+int launch_cta128(const float* a, float* l, const MatrixList& ml, int32_t* info, cudaStream_t s);
+
+// Blocked right-looking path for n > 128 (potrf_blocked.cu).
+size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode);
+int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
+                  size_t ws_bytes, int32_t* info, cudaStream_t s);
+
+// Cholesky adjoint (potrf_backward.cu).
+size_t backward_workspace_bytes(int64_t batch, int64_t n);
+int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, void* ws,
+                   size_t ws_bytes, cudaStream_t s);
+
+// Kernel ids reported by the launch trace (b2p_kernel_name).
+enum KernelId {
+  kKWarp32 = 0,
+  kKCta128,
+  kKCopyLower,
+  kKDiag,
+  kKPanel,
+  kKTrail,
+  kKTrailTc,
+  kKPanelTc,
+  kKSplit,
+  kKRagged,
+  kKBwdGemm,
+  kKBwdTrsm,
+  kKBwdSym,
+  kKCount
+};
+
+// RAII bracket: records a start/end CUDA event pair around one launch on
+// stream `s` while the trace is enabled; a no-op otherwise.
+class TraceScope {
+ public:
+  TraceScope(int kernel_id, cudaStream_t s);
+  ~TraceScope();
+
+ private:
+  int slot_;
+  cudaStream_t s_;
+};
+
+// Slots for ensure_smem_attr (one per kernel that needs > 48 KB).
+enum SmemSlot {
+  kSlotCta128 = 0,
+  kSlotDiag,
+  kSlotPanel,
+  kSlotTrail,
+  kSlotBwd0,
+  kSlotBwd1,
+  kSlotBwd2,
+  kSlotTc0,
+  kSlotTc1,
+  kSlotTc2,
+  kSlotTc3,
+  kSlotCount
+};
+
+}  // namespace b2p

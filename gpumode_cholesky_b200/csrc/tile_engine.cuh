@@ -1,0 +1,290 @@
+// Register/shared-memory Cholesky building blocks shared by every path.
+//
+//  * warp_factor32: one warp factors a 32x32 block held one row per lane in
+//    registers (right-looking, column by column).  The pivot column crosses
+//    lanes through a double-buffered 32-float shared array, so one
+//    __syncwarp per pivot orders it.
+//  * smem_potrf:    a CTA factors an n x n (n <= 128) matrix resident in
+//    shared memory, blocked by 32: warp 0 factors the diagonal block, every
+//    thread solves one panel row against it, then 4x4 register tiles apply
+//    the rank-32 trailing update to the lower triangle.
+//  * smem_trtri:    in-place-safe inverse of the lower-triangular factor in
+//    shared memory (n <= 128), blocked by 32; used by the blocked path to
+//    turn the panel TRSM into a GEMM.
+//
+// The algorithm is the textbook right-looking Cholesky that LAPACK's potrf
+// (called by the reference's ref_kernel, reference/reference.py:129-130, and
+// its cuSOLVER routes, submission.py:4268) computes; pivots use a refined
+// reciprocal square root instead of a divide.
+#pragma once
+
+#include "common.cuh"
+
+namespace b2p {
+
+// Transposed 32x32 copy of the current diagonal block's L, row stride 36.
+constexpr int kLtLd = 36;
+
+// Factor the 32x32 block x[] (row `lane`), columns >= w / rows >= w are
+// identity padding.  On return x holds L (lower part valid, upper part is
+// don't-care) and inv_pivot holds 1/L[lane][lane].  Returns the first local
+// pivot index that was not positive, or -1.  All 32 lanes must call.
+__device__ __forceinline__ int warp_factor32(float (&x)[32], int lane, int w, float* colbuf,
+                                             float& inv_pivot) {
+  int bad = -1;
+  inv_pivot = 1.0f;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    if (k < w) {  // warp-uniform
+      const float d = __shfl_sync(kFullMask, x[k], k);
+      if (bad < 0 && pivot_bad(d)) bad = k;
+      const float y = rsqrt_refined(d);
+      if (lane == k) inv_pivot = y;
+      x[k] = (lane == k) ? d * y : x[k] * y;
+      float* cb = colbuf + (k & 1) * 32;
+      cb[lane] = x[k];
+      __syncwarp();
+      // x[j] -= L[lane][k] * L[j][k] for j > k (upper part is don't-care).
+#pragma unroll
+      for (int j4 = (k + 1) / 4; j4 < 8; ++j4) {
+        const float4 c = reinterpret_cast<const float4*>(cb)[j4];
+        const float cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int j = 4 * j4 + e;
+          if (j > k) x[j] = fmaf(-x[k], cv[e], x[j]);
+        }
+      }
+    }
+  }
+  return bad;
+}
+
+// Scratch layout for smem_potrf / smem_trtri (floats).
+struct TileScratch {
+  float* lt;      // [32][kLtLd]   transposed L of the current diagonal block
+  float* invd;    // [128]         1/L[i][i]
+  float* pt;      // [32][ldpt]    transposed panel below the diagonal block
+  float* colbuf;  // [64]          warp_factor32 pivot column (double buffer)
+  int* flag;      // [1]           first bad pivot (global index) or -1
+  int ldpt;
+};
+
+__host__ __device__ constexpr int tile_scratch_floats(int ldpt) {
+  return 32 * kLtLd + 128 + 32 * ldpt + 64 + 4;
+}
+
+__device__ __forceinline__ TileScratch make_scratch(float* base, int ldpt) {
+  TileScratch s;
+  s.lt = base;
+  s.invd = s.lt + 32 * kLtLd;
+  s.pt = s.invd + 128;
+  s.colbuf = s.pt + 32 * ldpt;
+  s.flag = reinterpret_cast<int*>(s.colbuf + 64);
+  s.ldpt = ldpt;
+  return s;
+}
+
+// Factor the n x n SPD matrix in shared memory S (row stride lds, a multiple
+// of 4; lower triangle read, L written to the lower triangle, zeros written
+// to the upper part of each diagonal block only).  n <= 128.  All NT threads
+// call it; returns the first bad pivot (0-based) or -1, uniform across the CTA.
+template <int NT>
+__device__ int smem_potrf(float* S, int n, int lds, const TileScratch& sc) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  if (tid == 0) *sc.flag = -1;
+  for (int kb = 0; kb < n; kb += 32) {
+    const int w = min(32, n - kb);
+    if (warp == 0) {
+      float x[32];
+      const float* row = S + (size_t)(kb + lane) * lds + kb;
+#pragma unroll
+      for (int c4 = 0; c4 < 8; ++c4) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (lane < w && 4 * c4 < w) v = reinterpret_cast<const float4*>(row)[c4];
+        x[4 * c4 + 0] = v.x;
+        x[4 * c4 + 1] = v.y;
+        x[4 * c4 + 2] = v.z;
+        x[4 * c4 + 3] = v.w;
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        if (lane >= w || j >= w) x[j] = (lane == j) ? 1.0f : 0.0f;
+      }
+      float ip;
+      const int bad = warp_factor32(x, lane, w, sc.colbuf, ip);
+      if (lane == 0 && bad >= 0 && *sc.flag < 0) *sc.flag = kb + bad;
+      sc.invd[kb + lane] = ip;
+      float* srow = S + (size_t)(kb + lane) * lds + kb;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const float v = (j <= lane) ? x[j] : 0.0f;
+        if (lane < w && j < w) srow[j] = v;
+        sc.lt[j * kLtLd + lane] = (lane < w) ? v : 0.0f;
+      }
+    }
+    __syncthreads();
+    const int r0 = kb + 32;
+    const int R = n - r0;
+    if (R > 0) {
+      // Panel solve X * L_kk^T = P, one row per thread.
+      for (int t = tid; t < R; t += NT) {
+        float x[32];
+        const float* row = S + (size_t)(r0 + t) * lds + kb;
+#pragma unroll
+        for (int c4 = 0; c4 < 8; ++c4) {
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (4 * c4 < w) v = reinterpret_cast<const float4*>(row)[c4];
+          x[4 * c4 + 0] = v.x;
+          x[4 * c4 + 1] = v.y;
+          x[4 * c4 + 2] = v.z;
+          x[4 * c4 + 3] = v.w;
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (j >= w) x[j] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 32; ++m) {
+          x[m] *= sc.invd[kb + m];
+#pragma unroll
+          for (int j4 = (m + 1) / 4; j4 < 8; ++j4) {
+            const float4 c = reinterpret_cast<const float4*>(sc.lt + m * kLtLd)[j4];
+            const float cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int j = 4 * j4 + e;
+              if (j > m) x[j] = fmaf(-x[m], cv[e], x[j]);
+            }
+          }
+        }
+        float* wrow = S + (size_t)(r0 + t) * lds + kb;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          if (j < w) wrow[j] = x[j];
+          sc.pt[j * sc.ldpt + t] = x[j];
+        }
+      }
+      // Zero the transposed-panel padding so 4-wide tiles read finite values.
+      for (int t = R + tid; t < ((R + 3) & ~3); t += NT) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) sc.pt[j * sc.ldpt + t] = 0.0f;
+      }
+      __syncthreads();
+      // Trailing update S[i][j] -= sum_m P[i][m] P[j][m], i >= j >= r0.
+      const int T4 = (R + 3) >> 2;
+      const int ntiles = T4 * (T4 + 1) / 2;
+      for (int q = tid; q < ntiles; q += NT) {
+        int ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+        while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
+        while (ti * (ti + 1) / 2 > q) --ti;
+        const int tj = q - ti * (ti + 1) / 2;
+        float acc[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
+        for (int m = 0; m < w; ++m) {
+          const float4 a = reinterpret_cast<const float4*>(sc.pt + m * sc.ldpt)[ti];
+          const float4 b = reinterpret_cast<const float4*>(sc.pt + m * sc.ldpt)[tj];
+          const float av[4] = {a.x, a.y, a.z, a.w};
+          const float bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = 4 * ti + r;
+          if (i < R) {
+            float* srow = S + (size_t)(r0 + i) * lds + r0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const int j = 4 * tj + c;
+              if (j <= i) srow[j] -= acc[r][c];
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  return *sc.flag;
+}
+
+// Inverse T = L^{-1} of the lower-triangular n x n factor in S (row stride
+// lds), written to Tm (row stride ldt, lower triangle + zero upper).  Uses
+// sc.invd from the preceding smem_potrf.  n <= 128, NT >= 128.
+//   diagonal 32-blocks: lane c of warp b forward-substitutes column c;
+//   off-diagonal blocks by block distance d: T_ij = -T_ii * sum_k L_ik T_kj.
+template <int NT>
+__device__ void smem_trtri(const float* S, int n, int lds, float* Tm, int ldt,
+                           const TileScratch& sc, float* work /* [4][32][33] */) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nblk = (n + 31) / 32;
+  // Zero the whole target first (upper part and padding stay zero).
+  for (int e = tid; e < n * ldt; e += NT) Tm[e] = 0.0f;
+  __syncthreads();
+  if (warp < nblk) {
+    const int kb = warp * 32;
+    const int w = min(32, n - kb);
+    const int c = lane;
+    float x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = (j == c) ? 1.0f : 0.0f;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      if (m < w) {
+        x[m] *= sc.invd[kb + m];
+#pragma unroll
+        for (int j = m + 1; j < 32; ++j) {
+          if (j < w) x[j] = fmaf(-S[(size_t)(kb + j) * lds + kb + m], x[m], x[j]);
+        }
+      }
+    }
+    if (c < w) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (j < w && j >= c) Tm[(size_t)(kb + j) * ldt + kb + c] = x[j];
+    }
+  }
+  __syncthreads();
+  for (int d = 1; d < nblk; ++d) {
+    // W_(ib) = sum_{k=jb}^{ib-1} L_(ib,k) T_(k,jb) for every pair at distance d.
+    const int npairs = nblk - d;
+    for (int e = tid; e < npairs * 1024; e += NT) {
+      const int p = e >> 10;
+      const int r = (e >> 5) & 31;
+      const int cc = e & 31;
+      const int jb = p, ib = p + d;
+      const int i = ib * 32 + r, j = jb * 32 + cc;
+      float s = 0.0f;
+      if (i < n && j < n) {
+        const int kend = ib * 32;
+        for (int k = jb * 32; k < kend; ++k) s = fmaf(S[(size_t)i * lds + k], Tm[(size_t)k * ldt + j], s);
+      }
+      work[(p * 32 + r) * 33 + cc] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < npairs * 1024; e += NT) {
+      const int p = e >> 10;
+      const int r = (e >> 5) & 31;
+      const int cc = e & 31;
+      const int jb = p, ib = p + d;
+      const int i = ib * 32 + r, j = jb * 32 + cc;
+      if (i < n && j < n) {
+        float s = 0.0f;
+        for (int k = 0; k <= r; ++k) s = fmaf(Tm[(size_t)i * ldt + ib * 32 + k], work[(p * 32 + k) * 33 + cc], s);
+        Tm[(size_t)i * ldt + j] = -s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace b2p

@@ -1,0 +1,108 @@
+"""Host side of the batched Cholesky: the reference-facing ``custom_kernel``.
+
+``custom_kernel(data) -> output`` keeps the reference's contract
+(submission.py:4101-4268, reference/task.py:6-7, reference/eval.py:107-113):
+``data`` is a (batch, n, n) FP32 CUDA tensor of SPD matrices, never mutated;
+the result is a fresh tensor of the same shape, dtype and device holding L
+(lower triangle, positive diagonal, exact zeros above).  Unlike the reference
+there is no CPU path and no cuSOLVER fallback: a non-CUDA or non-FP32 input
+raises, and a failing library call raises :class:`PotrfError`.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+
+_WS: dict[tuple[int, int], torch.Tensor] = {}
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def workspace(device: torch.device, nbytes: int) -> torch.Tensor:
+    """Per-(device, stream) scratch buffer grown on demand, 256-byte aligned.
+
+    Calls that share a stream are ordered by it, so one buffer per stream is
+    safe; callers running several streams get one buffer each.
+    """
+    key = (device.index if device.index is not None else torch.cuda.current_device(), _stream_ptr(device))
+    buf = _WS.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+        _WS[key] = buf
+    return buf
+
+
+def resolve_mode(mode: str | int | None, n: int) -> int:
+    """Precision mode code for order n; None picks the library default (FP32)."""
+    if mode is None:
+        return _lib.MODE_FP32
+    if isinstance(mode, int):
+        return mode
+    flags = 0
+    name = mode.lower()
+    if name.endswith("+fp64diag"):
+        flags = _lib.FLAG_FP64_DIAG
+        name = name[: -len("+fp64diag")]
+    if name not in _lib.MODES:
+        raise ValueError(f"unknown precision mode {mode!r}; expected one of {sorted(_lib.MODES)}")
+    return _lib.MODES[name] | flags
+
+
+def _check_input(a: torch.Tensor) -> None:
+    if not isinstance(a, torch.Tensor):
+        raise TypeError("input must be a torch.Tensor")
+    if a.dim() != 3 or a.shape[-1] != a.shape[-2]:
+        raise ValueError(f"input must have shape (batch, n, n), got {tuple(a.shape)}")
+    if a.dtype != torch.float32:
+        raise TypeError(f"input dtype must be torch.float32, got {a.dtype}")
+    if not a.is_cuda:
+        raise RuntimeError("input must be a CUDA tensor: this library has no CPU path")
+
+
+def cholesky(
+    a: torch.Tensor,
+    mode: str | int | None = None,
+    out: torch.Tensor | None = None,
+    info: torch.Tensor | None = None,
+) -> torch.Tensor:
+    """Factor a batch of SPD matrices: returns L with A = L L^T.
+
+    ``mode`` selects the trailing-update arithmetic ("fp32", "tf32",
+    "bf16x3", "fp8", optionally suffixed "+fp64diag").  ``info`` may be an
+    int32 CUDA tensor of shape (batch,) that receives 0 or the 1-based index
+    of the first non-positive pivot.
+    """
+    _check_input(a)
+    a = a.contiguous()
+    batch, n, _ = a.shape
+    code = resolve_mode(mode, n)
+    if out is None:
+        out = torch.empty_like(a)
+    elif out.shape != a.shape or out.dtype != torch.float32 or not out.is_contiguous() or out.device != a.device:
+        raise ValueError("out must be a contiguous float32 tensor shaped like the input, on the same device")
+    lib = _lib.load()
+    with torch.cuda.device(a.device):
+        ws_bytes = lib.b2p_potrf_workspace_size(batch, n, code)
+        ws_ptr = workspace(a.device, ws_bytes).data_ptr() if ws_bytes else None
+        info_ptr = None
+        if info is not None:
+            if info.dtype != torch.int32 or info.numel() < batch or not info.is_cuda:
+                raise ValueError("info must be an int32 CUDA tensor with at least batch elements")
+            info_ptr = info.data_ptr()
+        st = lib.b2p_potrf_batched(
+            a.data_ptr(), out.data_ptr(), batch, n, code, ws_ptr, ws_bytes, info_ptr, _stream_ptr(a.device)
+        )
+    _lib.check(st, "b2p_potrf_batched")
+    return out
+
+
+def custom_kernel(data: torch.Tensor) -> torch.Tensor:
+    """Drop-in for the reference entry point ``custom_kernel`` (submission.py:4101).
+
+    One library call on the current stream, no host synchronisation.
+    """
+    return cholesky(data)

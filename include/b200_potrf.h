@@ -1,0 +1,133 @@
+/*
+ * b200_potrf.h -- C ABI of the B200 batched Cholesky (potrf) library.
+ *
+ * The library factors SPD matrices A = L L^T on an NVIDIA B200 (sm_100a).
+ * All buffers are device pointers owned by the caller; the library allocates
+ * nothing on its own and keeps no state between calls except read-only
+ * tables.  Every entry point returns an int status (B2P_OK on success) and
+ * never aborts; b2p_status_string() and b2p_last_error() describe failures.
+ * Work is enqueued on the caller's stream (a cudaStream_t passed as void*;
+ * NULL means the legacy default stream) and nothing synchronises the host,
+ * so every call can be captured in a CUDA graph.
+ *
+ * Layout: a batch of `batch` matrices, each n x n, FP32, row-major and
+ * contiguous (matrix b starts at element b*n*n).  The output holds L in the
+ * lower triangle, a strictly positive diagonal and exact zeros above it.
+ * The input is never written.
+ *
+ * Reference interface replaced (binga/gpumode_cholesky):
+ *   custom_kernel(data) -> output   submission.py:4101-4268
+ *   ref_kernel / output contract    reference/reference.py:129-188
+ */
+#ifndef B200_POTRF_H_
+#define B200_POTRF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define B2P_API __attribute__((visibility("default")))
+#else
+#define B2P_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define B2P_OK 0
+#define B2P_ERR_INVALID_ARG 1   /* bad size, null pointer, misaligned buffer  */
+#define B2P_ERR_UNSUPPORTED 2   /* mode/size combination not implemented      */
+#define B2P_ERR_WORKSPACE 3     /* workspace missing or smaller than required */
+#define B2P_ERR_CUDA 4          /* a CUDA runtime call or launch failed       */
+#define B2P_ERR_TIMEOUT 5       /* a bounded device-side wait gave up         */
+
+/* ---- precision modes ------------------------------------------------------ *
+ * The diagonal tiles and the panel solves are FP32 in every mode; the mode
+ * selects the arithmetic of the trailing (Schur complement) updates.        */
+#define B2P_MODE_FP32 0    /* plain FP32 end to end (SIMT FMA)                 */
+#define B2P_MODE_TF32 1    /* trailing update on tcgen05 kind::tf32            */
+#define B2P_MODE_BF16X3 2  /* trailing update as hi*hi+hi*lo+lo*hi BF16 on tcgen05 */
+#define B2P_MODE_FP8 3     /* trailing update in per-tile scaled E4M3 (n>=16384) */
+#define B2P_MODE_MASK 0xff
+/* Flag OR-ed into the mode: factor diagonal tiles in FP64 and re-factor a
+ * panel in plain FP32 when its FP64 residual check fails.                    */
+#define B2P_FLAG_FP64_DIAG 0x100
+
+/* Library version as major*10000 + minor*100 + patch. */
+B2P_API int b2p_version(void);
+
+/* Static description of a status code. */
+B2P_API const char* b2p_status_string(int status);
+
+/* Detail message of the last failing call on this host thread ("" if none). */
+B2P_API const char* b2p_last_error(void);
+
+/* Bytes of device workspace b2p_potrf_batched needs (0 for n <= 128). */
+B2P_API size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode);
+
+/*
+ * Batched dense factorization.  Replaces custom_kernel(data) -> output
+ * (submission.py:4101-4268) for a contiguous FP32 (batch, n, n) CUDA tensor.
+ *   a, l       device pointers, batch*n*n floats each, 16-byte aligned; must
+ *              not overlap.
+ *   mode       B2P_MODE_* optionally OR-ed with B2P_FLAG_FP64_DIAG.
+ *   workspace  device scratch of at least b2p_potrf_workspace_size() bytes
+ *              (may be NULL when that size is 0), 256-byte aligned.
+ *   info       optional device int32[batch]: 0 on success, k+1 when the
+ *              k-th pivot was not positive (cuSOLVER potrf convention).  A
+ *              non-SPD matrix yields NaN from the failing column on.
+ *   stream     cudaStream_t (as void*).
+ */
+B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mode,
+                      void* workspace, size_t workspace_bytes, int32_t* info,
+                      void* stream);
+
+/*
+ * Ragged batch: `count` matrices of individual order n_host[i] packed in one
+ * buffer, matrix i starting at element offsets_host[i] (each row-major,
+ * contiguous, n_i*n_i floats, offsets multiples of 4).  The host arrays are
+ * read during the call only to size the schedule; the device copies
+ * (offsets_dev, n_dev, same contents) are what the kernels read, so the call
+ * can be replayed from a CUDA graph.  No counterpart exists in the reference
+ * (its dispatcher routes exact (batch, n) shapes only, submission.py:4111-4268).
+ */
+B2P_API size_t b2p_potrf_ragged_workspace_size(const int32_t* n_host, int64_t count, int mode);
+B2P_API int b2p_potrf_ragged(const float* a, float* l, const int64_t* offsets_host,
+                     const int32_t* n_host, const int64_t* offsets_dev,
+                     const int32_t* n_dev, int64_t count, int mode, void* workspace,
+                     size_t workspace_bytes, int32_t* info, void* stream);
+
+/*
+ * Cholesky adjoint: given L (output of the factorization) and Lbar = dLoss/dL
+ * (lower triangle used), writes Abar = dLoss/dA, symmetric:
+ *   P = Phi(L^T Lbar)  (lower triangle, diagonal halved)
+ *   Abar = 1/2 (S + S^T),  S = L^{-T} P L^{-1}.
+ * No counterpart exists in the reference (forward only); the oracle is
+ * torch.linalg.cholesky's autograd and FP64 finite differences.
+ */
+B2P_API size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n);
+B2P_API int b2p_potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch,
+                       int64_t n, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Launch trace: when enabled, every kernel the library launches is bracketed
+ * by a pair of CUDA events recorded on its launch stream, so a caller can
+ * read per-kernel device time (the counterpart of the reference's in-kernel
+ * clock64 phase profiler, submission.py:4711-4716,4991-4996).
+ *   b2p_trace_enable(capacity)  start recording up to `capacity` launches
+ *                               (0 stops recording and frees the events);
+ *   b2p_trace_read(ids, ms, max) synchronises the recorded events and writes
+ *                               kernel ids and durations; returns the count;
+ *   b2p_kernel_name(id)         the kernel's name.
+ */
+B2P_API int b2p_trace_enable(int capacity);
+B2P_API int b2p_trace_read(int32_t* kernel_ids, float* ms, int max_entries);
+B2P_API const char* b2p_kernel_name(int id);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200_POTRF_H_ */

@@ -1,0 +1,98 @@
+"""CPU: the C-ABI library builds, loads and exports every declared symbol.
+
+No compute call is made here (there is no GPU); only entry points that
+return before touching the device are exercised.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from gpumode_cholesky_b200 import _lib, build
+from gpumode_cholesky_b200.potrf import resolve_mode
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        names |= set(re.findall(r"B2P_API\s+[\w\s\*]+?\b(b2p_\w+)\s*\(", h.read_text()))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = _declared_symbols()
+    assert {"b2p_potrf_batched", "b2p_potrf_ragged", "b2p_potrf_backward", "b2p_potrf_workspace_size"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    build.build()
+    out = subprocess.run(["nm", "-D", "--defined-only", str(build.LIB_PATH)], capture_output=True, text=True, check=True)
+    exported = {line.split()[-1] for line in out.stdout.splitlines() if " T " in line}
+    missing = _declared_symbols() - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+    assert set(_lib.SIGNATURES) == _declared_symbols()
+
+
+def test_library_loads_and_reports_version():
+    lib = _lib.load()
+    assert lib.b2p_version() >= 100
+    assert lib.b2p_status_string(_lib.B2P_OK) == b"ok"
+    assert lib.b2p_status_string(_lib.B2P_ERR_WORKSPACE).startswith(b"workspace")
+    assert lib.b2p_status_string(99) == b"unknown status"
+
+
+def test_argument_validation_without_device():
+    lib = _lib.load()
+    # empty batch: nothing to do, no device call
+    assert lib.b2p_potrf_batched(None, None, 0, 32, 0, None, 0, None, None) == _lib.B2P_OK
+    # negative sizes and unknown modes are rejected before any CUDA call
+    assert lib.b2p_potrf_batched(None, None, -1, 32, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_potrf_batched(None, None, 1, -3, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_potrf_batched(None, None, 1, 32, 0x77, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert b"mode" in lib.b2p_last_error()
+    assert lib.b2p_potrf_batched(None, None, 1, 32, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    # misaligned pointers
+    assert lib.b2p_potrf_batched(ctypes.c_void_p(8), ctypes.c_void_p(4096), 1, 32, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    # overlapping buffers
+    assert lib.b2p_potrf_batched(ctypes.c_void_p(4096), ctypes.c_void_p(4096 + 64), 1, 32, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert b"overlap" in lib.b2p_last_error()
+
+
+def test_workspace_sizes_are_host_only():
+    lib = _lib.load()
+    assert lib.b2p_potrf_workspace_size(4096, 32, 0) == 0
+    assert lib.b2p_potrf_workspace_size(256, 128, 0) == 0
+    assert lib.b2p_potrf_workspace_size(640, 512, 0) >= 640 * 64 * 64 * 4
+    assert lib.b2p_potrf_workspace_size(0, 512, 0) == 0
+
+
+def test_error_raises_python_exception():
+    with pytest.raises(_lib.PotrfError) as ei:
+        _lib.check(_lib.B2P_ERR_UNSUPPORTED, "call")
+    assert ei.value.status == _lib.B2P_ERR_UNSUPPORTED
+
+
+def test_mode_names():
+    assert resolve_mode(None, 512) == _lib.MODE_FP32
+    assert resolve_mode("bf16x3", 512) == _lib.MODE_BF16X3
+    assert resolve_mode("tf32+fp64diag", 512) == _lib.MODE_TF32 | _lib.FLAG_FP64_DIAG
+    with pytest.raises(ValueError):
+        resolve_mode("int8", 512)
+
+
+def test_custom_kernel_rejects_cpu_input():
+    import torch
+
+    from gpumode_cholesky_b200 import custom_kernel
+
+    with pytest.raises(RuntimeError, match="no CPU path"):
+        custom_kernel(torch.eye(4).expand(2, 4, 4).contiguous())
+    with pytest.raises(TypeError):
+        custom_kernel(torch.eye(4, dtype=torch.float64).expand(2, 4, 4).contiguous())

@@ -1,0 +1,104 @@
+"""GPU parity of the dense entry point against the oracle and the reference's golden outputs.
+
+Tolerances (FP32 factorization of FP32 input):
+  * the restated reference checker must pass (scaled residual <= 20);
+  * ||L - L64||_F / ||L64||_F <= 4 * (the reference's own error) + 1e-6, where
+    L64 is the FP64 oracle factor and the reference's error is that of its
+    golden L -- the library may differ from LAPACK only by rounding order;
+  * exact zeros above the diagonal, bitwise-identical repeats.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from gpumode_cholesky_b200 import cholesky, custom_kernel, inputs
+from tests.conftest import GOLDEN_CASES, case_id
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel_err(l, l64):
+    b = l.shape[0]
+    return np.linalg.norm((l - l64).reshape(b, -1), axis=1) / np.linalg.norm(l64.reshape(b, -1), axis=1)
+
+
+@pytest.mark.parametrize("c", GOLDEN_CASES, ids=case_id)
+def test_golden_parity(c):
+    a = torch.from_numpy(c["a"]).cuda()
+    a_copy = a.clone()
+    info = torch.full((c["batch"],), -7, dtype=torch.int32, device="cuda")
+    l = cholesky(a, info=info)
+    torch.cuda.synchronize()
+    assert torch.equal(a, a_copy), "input was mutated"
+    ln = l.cpu().numpy()
+    ok, msg = oracle.check_implementation(c["a"], ln)
+    assert ok, msg
+    assert np.all(np.triu(ln, 1) == 0.0)
+    assert np.array_equal(info.cpu().numpy(), c["info"])
+    l64, _ = oracle.potrf_f64(c["a"])
+    ours = _rel_err(ln, l64).max()
+    ref = _rel_err(c["l"], l64).max()
+    assert ours <= 4.0 * ref + 1e-6, (ours, ref)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 16, 31, 32, 33, 48, 64, 96, 127, 128, 129, 150, 192, 255, 256, 257, 384, 513])
+def test_orders_against_oracle(n):
+    batch = 3
+    a = inputs.generate_input(batch, n, 2, 1000 + n, "dense", device="cpu")
+    l = custom_kernel(a.cuda()).cpu().numpy()
+    ok, msg = oracle.check_implementation(a.numpy(), l)
+    assert ok, msg
+    l64, _ = oracle.potrf_f64(a.numpy())
+    assert _rel_err(l, l64).max() < 2e-5
+
+
+def test_repeat_is_bitwise_identical():
+    a = inputs.generate_input(64, 200, 2, 5, "dense", device="cpu").cuda()
+    l1 = custom_kernel(a)
+    l2 = custom_kernel(a)
+    l3 = custom_kernel(a.clone())
+    assert torch.equal(l1, l2) and torch.equal(l1, l3)
+
+
+def test_fresh_output_per_call():
+    a = inputs.generate_input(8, 32, 2, 6, "dense", device="cpu").cuda()
+    l1 = custom_kernel(a)
+    l2 = custom_kernel(a)
+    assert l1.data_ptr() != l2.data_ptr()
+
+
+def test_nonspd_reports_info(golden_nonspd):
+    a, info_ref = golden_nonspd
+    info = torch.zeros(a.shape[0], dtype=torch.int32, device="cuda")
+    l = cholesky(torch.from_numpy(a).cuda(), info=info)
+    assert np.array_equal(info.cpu().numpy(), info_ref)
+    ln = l.cpu().numpy()
+    assert np.isfinite(ln[0]).all() and np.isnan(ln[1]).any()
+
+
+@pytest.mark.parametrize("n", [32, 100, 300])
+def test_nonspd_info_all_paths(n):
+    a = inputs.generate_input(2, n, 2, 55, "dense", device="cpu")
+    k = n // 2 + 1
+    a[1, k, k] = -5.0
+    _, ref = oracle.potrf_f64(a.numpy())
+    info = torch.zeros(2, dtype=torch.int32, device="cuda")
+    cholesky(a.cuda(), info=info)
+    assert info.cpu().tolist() == ref.tolist()
+
+
+@pytest.mark.parametrize("batch,n", [(4096, 32), (1024, 64), (256, 128), (640, 512), (60, 1024), (8, 2048)])
+def test_full_size_properties(batch, n):
+    """Benchmark shapes: relative residual in FP64 on the device, triangularity, positive diagonal."""
+    a = inputs.well_conditioned(batch, n, seed=n, device="cuda")
+    l = custom_kernel(a)
+    assert torch.isfinite(l).all()
+    assert (torch.triu(l, 1) == 0).all()
+    assert (torch.diagonal(l, dim1=-2, dim2=-1) > 0).all()
+    ld = l.double()
+    r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - a.double()) / torch.linalg.matrix_norm(a.double())
+    assert r.max().item() < 2e-6
