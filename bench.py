@@ -53,7 +53,7 @@ def _flops(batch: int, n: int) -> float:
 def _clock_sampler_start(gpu_index: int):
     path = tempfile.NamedTemporaryFile(prefix="clocks", suffix=".csv", delete=False).name
     q = (
-        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
     )
@@ -69,7 +69,10 @@ def _clock_sampler_start(gpu_index: int):
         return None, None, path
 
 
-def _clock_sampler_stop(state) -> dict:
+def _clock_sampler_stop(state, t0: float, t1: float) -> dict:
+    """Median SM clock and throttle reasons of the samples taken in [t0, t1] (host time)."""
+    import datetime as _dt
+
     p, f, path = state
     if p is None:
         return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -79,26 +82,29 @@ def _clock_sampler_stop(state) -> dict:
     except Exception:
         p.kill()
     f.close()
-    sms, maxs, reasons = [], [], set()
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    rows = []
     for line in Path(path).read_text().splitlines():
         parts = [x.strip() for x in line.split(",")]
         if len(parts) < 9:
             continue
         try:
-            sms.append(float(parts[1]))
-            maxs.append(float(parts[2]))
+            ts = _dt.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            rows.append((ts, float(parts[1]), float(parts[2]), parts[5:9]))
         except ValueError:
             continue
-        for nm, v in zip(names, parts[5:9]):
-            if v.lower() == "active":
-                reasons.add(nm)
     os.unlink(path)
-    sms.sort()
+    window = [r for r in rows if t0 - 0.05 <= r[0] <= t1 + 0.05]
+    label = "timed region"
+    if not window:
+        window, label = rows, "whole run (timed region shorter than the sampling period)"
+    sms = sorted(r[1] for r in window)
+    reasons = {nm for r in window for nm, v in zip(names, r[3]) if v.lower() == "active"}
     return {
         "sm_mhz": sms[len(sms) // 2] if sms else None,
-        "sm_max_mhz": max(maxs) if maxs else None,
+        "sm_max_mhz": max((r[2] for r in window), default=None),
         "samples": len(sms),
+        "window": label,
         "reasons": sorted(reasons),
     }
 
@@ -219,15 +225,18 @@ def run_ours(args) -> int:
 
             dist.barrier()
 
+    clk = _clock_sampler_start(local)
+    time.sleep(0.3)  # let nvidia-smi start sampling
     for _ in range(args.warmup):
         step(mode)
     barrier()
     torch.cuda.synchronize()
-    clk = _clock_sampler_start(local)
+    t_start = time.time()
     ms = timed(lambda: step(mode), args.steps)
     torch.cuda.synchronize()
+    t_end = time.time()
     barrier()
-    clocks = _clock_sampler_stop(clk)
+    clocks = _clock_sampler_stop(clk, t_start, t_end)
     if ws > 1:
         import torch.distributed as dist
 

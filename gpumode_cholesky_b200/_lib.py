@@ -40,6 +40,8 @@ SIGNATURES = {
         ctypes.c_int,
         [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
     ),
+    "b2p_noalloc_scratch_bytes": (_c_sz, []),
+    "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_potrf_ragged_workspace_size": (_c_sz, [_c_p, _c_i64, ctypes.c_int]),
     "b2p_potrf_ragged": (
         ctypes.c_int,

@@ -85,6 +85,24 @@ B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n
                       void* stream);
 
 /*
+ * Allocation-free variant of b2p_potrf_batched for callers that cannot
+ * allocate device memory (code inside an allocator-free region, a plugin
+ * whose host owns every device allocation, a serving process that forbids
+ * allocation after start-up).  It takes no workspace: the scratch of the
+ * blocked path lives in a 16 MiB device array inside this library, held by
+ * every GPU that loads it until the process exits
+ * (b2p_noalloc_scratch_bytes() reports the size).  A call needing more
+ * (batch * 16 KiB for n > 128, i.e. more than 1024 such matrices) is
+ * rejected with B2P_ERR_WORKSPACE.  Calls share the array: calls that overlap
+ * on the GPU race, so serialise them on one stream.  The first call on each
+ * device looks the array's address up (cudaGetSymbolAddress); make it before
+ * any stream capture.  No counterpart exists in the reference.
+ */
+B2P_API size_t b2p_noalloc_scratch_bytes(void);
+B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, int64_t n,
+                                      int mode, int32_t* info, void* stream);
+
+/*
  * Ragged batch: `count` matrices of individual order n_host[i] packed in one
  * buffer, matrix i starting at element offsets_host[i] (each row-major,
  * contiguous, n_i*n_i floats, offsets multiples of 4).  The host arrays are
