@@ -28,6 +28,10 @@ size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode);
 int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
                   size_t ws_bytes, int32_t* info, cudaStream_t s);
 
+// tcgen05 trailing update, TF32 or BF16x3 (syrk_tc.cu).
+int launch_syrk_tc(const float* csrc, float* l, int64_t batch, int n, int k0, int mode, int32_t* info,
+                   cudaStream_t s);
+
 // Cholesky adjoint (potrf_backward.cu).
 size_t backward_workspace_bytes(int64_t batch, int64_t n);
 int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, void* ws,

@@ -1,15 +1,22 @@
 // Blocked right-looking factorization for n > 128 (plain FP32 SIMT form).
 //
-// The output buffer holds the working matrix.  One copy pass writes tril(A)
-// into L (zeros above the diagonal), then for each 64-wide block column k0:
+// The output buffer holds the working matrix.  For each 64-wide block column
+// k0 three kernels run:
 //
-//   diag   one CTA per matrix: factor L[k0:k0+64, k0:k0+64] in shared memory
-//          (smem_potrf), invert it (smem_trtri), write L_kk back and
-//          T^T = inv(L_kk)^T to the workspace;
-//   panel  L[i, k0:k0+64] <- L[i, k0:k0+64] * T^T for the rows below
+//   diag   one CTA per matrix: factor the 64x64 diagonal block and invert it
+//          in shared memory (diag64.cuh); write L_kk (zeros above its
+//          diagonal), zero the strictly-upper strip to the right of the
+//          block, and store T^T = inv(L_kk)^T in the workspace;
+//   panel  L[i, k0:k0+64] <- A[i, k0:k0+64] * T^T for the rows below
 //          (the TRSM as a GEMM against the explicit inverse);
-//   trail  L[i, j] -= sum_m L[i, k0+m] L[j, k0+m] over the lower 64x64
-//          tiles of the trailing matrix (the SYRK).
+//   trail  C[i, j] -= sum_m L[i, k0+m] L[j, k0+m] over the lower 64x64 tiles
+//          of the trailing matrix (the SYRK).
+//
+// The first block column reads the caller's A directly (its diagonal block,
+// its panel and, in the first trailing update, every lower tile), so A's
+// lower triangle is read once and no separate copy pass runs; later steps
+// work in place on L.  Every element of L is written exactly once by the
+// step that finalises it, except the trailing tiles that later steps update.
 //
 // The reference reaches the same blocked schedule through cuSOLVER / cuBLAS
 // and Triton (submission.py:2375-2661 split32, 3217-3251 right-looking TF32,
@@ -17,173 +24,220 @@
 // a kernel of this library.
 #include <algorithm>
 
+#include "diag64.cuh"
 #include "launch.h"
-#include "tile_engine.cuh"
 
 namespace b2p {
 
-constexpr int kNB = 64;            // block column width
-constexpr int kTile = 64;          // panel rows / trailing tile edge per CTA
-constexpr int kBlkThreads = 256;
-constexpr int kDiagLd = kNB + 4;   // 68
-constexpr int kGemmLd = kTile + 4; // 68
+constexpr int kNB = 64;             // block column width
+constexpr int kTile = 64;           // panel rows / trailing tile edge per CTA
+constexpr int kGemmLd = kTile + 4;  // 68
 constexpr int kMaxGridY = 65535;
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // -------------------------------------------------------------------------
-// tril copy: L[i][j] = (j <= i) ? A[i][j] : 0, info[b] = 0.  One row per CTA
-// iteration, float4 columns when rows are 16-byte aligned.
-__global__ void __launch_bounds__(256) copy_lower_kernel(const float* __restrict__ a,
-                                                         float* __restrict__ l, int64_t batch,
-                                                         int n, int32_t* __restrict__ info) {
-  const int64_t rows = batch * (int64_t)n;
-  const bool vec = (n & 3) == 0;
-  for (int64_t g = blockIdx.x; g < rows; g += gridDim.x) {
-    const int64_t b = g / n;
-    const int r = (int)(g - b * n);
-    const float* src = a + g * n;
-    float* dst = l + g * n;
+// diag: factor + invert the 64x64 diagonal block of every matrix.
+__global__ void __launch_bounds__(kD64Threads, 4)
+    diag_kernel(const float* __restrict__ src, float* __restrict__ l, int64_t batch, int n, int k0,
+                float* __restrict__ tws, int32_t* __restrict__ info) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Diag64Smem& sm = *reinterpret_cast<Diag64Smem*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int w = min(kNB, n - k0);
+  const bool vec = (n & 3) == 0;  // then w is a multiple of 4 as well
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const size_t moff = (size_t)b * n * n + (size_t)k0 * n + k0;
+    const float* in = src + moff;
+    float* base = l + moff;
     if (vec) {
-      const int n4 = n >> 2;
-      for (int q = threadIdx.x; q < n4; q += blockDim.x) {
-        const int c = q * 4;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c <= r) {
-          v = __ldg(reinterpret_cast<const float4*>(src) + q);
-          if (c + 1 > r) v.y = 0.0f;
-          if (c + 2 > r) v.z = 0.0f;
-          if (c + 3 > r) v.w = 0.0f;
+      float4 v[8];
+#pragma unroll
+      for (int it = 0; it < 8; ++it) {
+        const int e4 = tid + kD64Threads * it;
+        const int r = e4 >> 4, c = (e4 & 15) * 4;
+        v[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < w && c <= r) v[it] = *reinterpret_cast<const float4*>(in + (size_t)r * n + c);
+      }
+#pragma unroll
+      for (int it = 0; it < 8; ++it) {
+        const int e4 = tid + kD64Threads * it;
+        const int r = e4 >> 4, c = (e4 & 15) * 4;
+        float e[4] = {v[it].x, v[it].y, v[it].z, v[it].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (c + q > r) e[q] = 0.0f;
+          if (r >= w) e[q] = (r == c + q) ? 1.0f : 0.0f;
         }
-        reinterpret_cast<float4*>(dst)[q] = v;
+        *reinterpret_cast<float4*>(sm.S + r * kD64Ld + c) = make_float4(e[0], e[1], e[2], e[3]);
       }
     } else {
-      for (int c = threadIdx.x; c < n; c += blockDim.x) dst[c] = (c <= r) ? __ldg(src + c) : 0.0f;
+      float v[32];
+#pragma unroll
+      for (int it = 0; it < 32; ++it) {
+        const int e = tid + kD64Threads * it;
+        const int r = e >> 6, c = e & 63;
+        v[it] = (r == c) ? 1.0f : 0.0f;
+        if (r < w && c <= r) v[it] = in[(size_t)r * n + c];
+        else if (r < w) v[it] = 0.0f;
+      }
+#pragma unroll
+      for (int it = 0; it < 32; ++it) {
+        const int e = tid + kD64Threads * it;
+        sm.S[(e >> 6) * kD64Ld + (e & 63)] = v[it];
+      }
     }
-    if (info != nullptr && r == 0 && threadIdx.x == 0) info[b] = 0;
-  }
-}
-
-// -------------------------------------------------------------------------
-constexpr size_t diag_smem_floats() {
-  return (size_t)2 * kNB * kDiagLd + tile_scratch_floats(kDiagLd) + 3 * 32 * 33;
-}
-
-__global__ void __launch_bounds__(kBlkThreads, 1)
-    diag_kernel(float* __restrict__ l, int64_t batch, int n, int k0, float* __restrict__ tws,
-                int32_t* __restrict__ info) {
-  extern __shared__ __align__(16) float smem[];
-  float* S = smem;
-  float* Tm = S + kNB * kDiagLd;
-  const TileScratch sc = make_scratch(Tm + kNB * kDiagLd, kDiagLd);
-  float* work = smem + 2 * kNB * kDiagLd + tile_scratch_floats(kDiagLd);
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-  const int w = min(kNB, n - k0);
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
-    float* base = l + b * (int64_t)n * n + (int64_t)k0 * n + k0;
-    for (int r = warp; r < w; r += kBlkThreads / 32)
-      for (int c = lane; c <= r; c += 32) S[r * kDiagLd + c] = base[(size_t)r * n + c];
     __syncthreads();
-    const int bad = smem_potrf<kBlkThreads>(S, w, kDiagLd, sc);
-    smem_trtri<kBlkThreads>(S, w, kDiagLd, Tm, kDiagLd, sc, work);
-    __syncthreads();
-    for (int r = warp; r < w; r += kBlkThreads / 32)
-      for (int c = lane; c <= r; c += 32) base[(size_t)r * n + c] = S[r * kDiagLd + c];
+    const int bad = diag64_factor_invert(sm);
+    // L_kk with zeros above its diagonal.
+    for (int e = tid; e < 64 * 64; e += kD64Threads) {
+      const int r = e >> 6, c = e & 63;
+      if (r < w && c < w) base[(size_t)r * n + c] = sm.S[r * kD64Ld + c];
+    }
+    // Strictly-upper strip right of the block: rows k0..k0+w, cols k0+64..n.
+    const int strip = n - k0 - kNB;
+    if (strip > 0) {
+      if (vec) {
+        const int s4 = strip >> 2;
+        for (int e = tid; e < w * s4; e += kD64Threads) {
+          const int r = e / s4, q = e - (e / s4) * s4;
+          reinterpret_cast<float4*>(base + (size_t)r * n + kNB)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      } else {
+        for (int e = tid; e < w * strip; e += kD64Threads) {
+          const int r = e / strip, c = e - (e / strip) * strip;
+          base[(size_t)r * n + kNB + c] = 0.0f;
+        }
+      }
+    }
     float* tb = tws + b * kNB * kNB;
-    for (int e = tid; e < kNB * kNB; e += kBlkThreads) {
-      const int m = e / kNB, c = e - (e / kNB) * kNB;
-      tb[e] = (m < w && c < w) ? Tm[c * kDiagLd + m] : 0.0f;  // T^T[m][c] = T[c][m]
+    for (int e = tid; e < kNB * kNB; e += kD64Threads) {
+      const int m = e >> 6, c = e & 63;
+      tb[e] = (m < w && c < w) ? sm.T[c * kD64Ld + m] : 0.0f;  // T^T[m][c] = T[c][m]
     }
-    if (info != nullptr && tid == 0 && bad >= 0 && info[b] == 0) info[b] = k0 + bad + 1;
+    if (info != nullptr && tid == 0) {
+      if (k0 == 0) info[b] = bad >= 0 ? bad + 1 : 0;
+      else if (bad >= 0 && info[b] == 0) info[b] = k0 + bad + 1;
+    }
     __syncthreads();
   }
 }
 
 // -------------------------------------------------------------------------
-// Load a kTile x kNB block of rows (row0.., cols col0..col0+kNB) of an n x n
-// matrix into dst[m][i] (transposed, row stride kGemmLd).  Rows >= n load 0.
+// 64x64 FP32 tile products with 64 threads, 8x8 outputs per thread.
+constexpr int kGemmThreads = 64;
+
+// Load rows row0..row0+63 (cols col0..col0+63) of an n x n matrix into
+// dst[m][i] (transposed, row stride kGemmLd).  Rows >= n load 0.  Every
+// load is issued before the first shared-memory store.
 __device__ __forceinline__ void load_rows_t(const float* __restrict__ mat, int n, int row0,
                                             int col0, float* dst) {
-  const int tid = threadIdx.x;
+  const int i = threadIdx.x;
+  const bool ok = row0 + i < n;
   if ((n & 3) == 0) {
-    constexpr int kQ = kNB / 4;
-    for (int e = tid; e < kTile * kQ; e += kBlkThreads) {
-      const int i = e / kQ, q = e - (e / kQ) * kQ;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (row0 + i < n)
-        v = reinterpret_cast<const float4*>(mat + (size_t)(row0 + i) * n + col0)[q];
-      dst[(4 * q + 0) * kGemmLd + i] = v.x;
-      dst[(4 * q + 1) * kGemmLd + i] = v.y;
-      dst[(4 * q + 2) * kGemmLd + i] = v.z;
-      dst[(4 * q + 3) * kGemmLd + i] = v.w;
+    const float4* src = reinterpret_cast<const float4*>(mat + (size_t)(ok ? row0 + i : 0) * n + col0);
+    float4 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = ok ? src[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      dst[(4 * q + 0) * kGemmLd + i] = v[q].x;
+      dst[(4 * q + 1) * kGemmLd + i] = v[q].y;
+      dst[(4 * q + 2) * kGemmLd + i] = v[q].z;
+      dst[(4 * q + 3) * kGemmLd + i] = v[q].w;
     }
   } else {
-    for (int e = tid; e < kTile * kNB; e += kBlkThreads) {
-      const int i = e / kNB, m = e - (e / kNB) * kNB;
-      dst[m * kGemmLd + i] = (row0 + i < n) ? mat[(size_t)(row0 + i) * n + col0 + m] : 0.0f;
-    }
+    const float* src = mat + (size_t)(ok ? row0 + i : 0) * n + col0;
+#pragma unroll 16
+    for (int m = 0; m < kNB; ++m) dst[m * kGemmLd + i] = ok ? src[m] : 0.0f;
   }
 }
 
-// acc[r][c] = sum_m As[m][4ty+r] * Bs[m][4tx+c]
-__device__ __forceinline__ void tile_mma_4x4(const float* As, const float* Bs, int ty, int tx,
-                                             float (&acc)[4][4]) {
+// Row/column owned by register slot r (0..7) of thread coordinate t (0..7):
+// {4t..4t+3} then {32+4t..32+4t+3}, so that the eight threads of a quarter
+// warp read 128 contiguous bytes (bank-conflict-free float4 loads).
+__device__ __forceinline__ int slot_index(int t, int r) { return (r < 4) ? 4 * t + r : 32 + 4 * t + (r - 4); }
+
+// acc[r][c] = sum_m As[m][slot(ty,r)] * Bs[m][slot(tx,c)]
+__device__ __forceinline__ void tile_mma_8x8(const float* As, const float* Bs, int ty, int tx,
+                                             float (&acc)[8][8]) {
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int r = 0; r < 8; ++r)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
-#pragma unroll 8
+    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
+#pragma unroll 4
   for (int m = 0; m < kNB; ++m) {
-    const float4 av = *reinterpret_cast<const float4*>(As + m * kGemmLd + 4 * ty);
-    const float4 bv = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 4 * tx);
-    const float a4[4] = {av.x, av.y, av.z, av.w};
-    const float b4[4] = {bv.x, bv.y, bv.z, bv.w};
+    const float4 a0 = *reinterpret_cast<const float4*>(As + m * kGemmLd + 4 * ty);
+    const float4 a1 = *reinterpret_cast<const float4*>(As + m * kGemmLd + 32 + 4 * ty);
+    const float4 b0 = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 4 * tx);
+    const float4 b1 = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 32 + 4 * tx);
+    const float a8[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float b8[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a4[r], b4[c], acc[r][c]);
+      for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(a8[r], b8[c], acc[r][c]);
   }
 }
 
-__global__ void __launch_bounds__(kBlkThreads)
-    panel_kernel(float* __restrict__ l, int64_t batch, int n, int k0,
+__global__ void __launch_bounds__(kGemmThreads)
+    panel_kernel(const float* __restrict__ src, float* __restrict__ l, int64_t batch, int n, int k0,
                  const float* __restrict__ tws) {
   __shared__ __align__(16) float Ps[kNB * kGemmLd];
   __shared__ __align__(16) float Ts[kNB * kGemmLd];
   const int tid = threadIdx.x;
-  const int ty = tid >> 4, tx = tid & 15;
+  const int ty = tid >> 3, tx = tid & 7;
   const int row0 = k0 + kNB + blockIdx.x * kTile;
   for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
-    float* mat = l + b * (int64_t)n * n;
-    load_rows_t(mat, n, row0, k0, Ps);
+    const size_t moff = (size_t)b * n * n;
     const float* tb = tws + b * kNB * kNB;
-    for (int e = tid; e < kNB * kNB / 4; e += kBlkThreads) {
-      const int m = e / (kNB / 4), q = e - (e / (kNB / 4)) * (kNB / 4);
-      *reinterpret_cast<float4*>(Ts + m * kGemmLd + 4 * q) =
-          __ldg(reinterpret_cast<const float4*>(tb + m * kNB) + q);
+#pragma unroll
+    for (int it = 0; it < 16; ++it) {
+      const int e = tid + kGemmThreads * it;
+      const int m = e >> 4, q = e & 15;
+      cp_async16(Ts + m * kGemmLd + 4 * q, tb + m * kNB + 4 * q);
     }
+    cp_async_commit();
+    load_rows_t(src + moff, n, row0, k0, Ps);
+    cp_async_wait_all();
     __syncthreads();
-    float acc[4][4];
-    tile_mma_4x4(Ps, Ts, ty, tx, acc);
+    float acc[8][8];
+    tile_mma_8x8(Ps, Ts, ty, tx, acc);
+    float* mat = l + moff;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = row0 + 4 * ty + r;
+    for (int r = 0; r < 8; ++r) {
+      const int i = row0 + slot_index(ty, r);
       if (i < n) {
-        float* dst = mat + (size_t)i * n + k0 + 4 * tx;
+        float* dst = mat + (size_t)i * n + k0;
+        if ((n & 3) == 0) {
+          reinterpret_cast<float4*>(dst + 4 * tx)[0] = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+          reinterpret_cast<float4*>(dst + 32 + 4 * tx)[0] = make_float4(acc[r][4], acc[r][5], acc[r][6], acc[r][7]);
+        } else {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) dst[c] = acc[r][c];
+          for (int c = 0; c < 8; ++c) dst[slot_index(tx, c)] = acc[r][c];
+        }
       }
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kBlkThreads)
-    trail_kernel(float* __restrict__ l, int64_t batch, int n, int k0) {
-  __shared__ __align__(16) float As[kNB * kGemmLd];
-  __shared__ __align__(16) float Bs[kNB * kGemmLd];
+// Trailing SYRK on lower 64x64 tiles.  The C tile is prefetched into shared
+// memory with cp.async while the panel tiles load and multiply; `csrc` is A
+// for the first block column and L afterwards, the result always goes to L.
+__global__ void __launch_bounds__(kGemmThreads)
+    trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, int64_t batch, int n, int k0) {
+  extern __shared__ __align__(16) float tsm[];
+  float* As = tsm;
+  float* Bs = As + kNB * kGemmLd;
+  float* Cs = Bs + kNB * kGemmLd;  // [64][kGemmLd], row-major C tile
   const int tid = threadIdx.x;
-  const int ty = tid >> 4, tx = tid & 15;
+  const int ty = tid >> 3, tx = tid & 7;
   const int q = blockIdx.x;
   int ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
   while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
@@ -191,22 +245,49 @@ __global__ void __launch_bounds__(kBlkThreads)
   const int tj = q - ti * (ti + 1) / 2;
   const int t0 = k0 + kNB;
   const int i0 = t0 + ti * kTile, j0 = t0 + tj * kTile;
+  const bool vec = (n & 3) == 0 && j0 + 64 <= n;
   for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
-    float* mat = l + b * (int64_t)n * n;
+    const size_t moff = (size_t)b * n * n;
+    if (vec) {
+#pragma unroll
+      for (int it = 0; it < 16; ++it) {
+        const int e = tid + kGemmThreads * it;
+        const int r = e >> 4, c4 = e & 15;
+        if (i0 + r < n) cp_async16(Cs + r * kGemmLd + 4 * c4, csrc + moff + (size_t)(i0 + r) * n + j0 + 4 * c4);
+      }
+      cp_async_commit();
+    }
+    float* mat = l + moff;
     load_rows_t(mat, n, i0, k0, As);
     if (ti != tj) load_rows_t(mat, n, j0, k0, Bs);
     __syncthreads();
-    float acc[4][4];
-    tile_mma_4x4(As, ti != tj ? Bs : As, ty, tx, acc);
+    float acc[8][8];
+    tile_mma_8x8(As, ti != tj ? Bs : As, ty, tx, acc);
+    if (vec) cp_async_wait_all();
+    __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = i0 + 4 * ty + r;
+    for (int r = 0; r < 8; ++r) {
+      const int rl = slot_index(ty, r);
+      const int i = i0 + rl;
       if (i < n) {
-        float* dst = mat + (size_t)i * n + j0 + 4 * tx;
+        float* row = mat + (size_t)i * n + j0;
+        if (vec && ti != tj) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int j = j0 + 4 * tx + c;
-          if (j <= i) dst[c] -= acc[r][c];
+          for (int h = 0; h < 2; ++h) {
+            float4 c = *reinterpret_cast<const float4*>(Cs + rl * kGemmLd + 32 * h + 4 * tx);
+            c.x -= acc[r][4 * h + 0];
+            c.y -= acc[r][4 * h + 1];
+            c.z -= acc[r][4 * h + 2];
+            c.w -= acc[r][4 * h + 3];
+            *reinterpret_cast<float4*>(row + 32 * h + 4 * tx) = c;
+          }
+        } else {
+          const float* crow = csrc + moff + (size_t)i * n + j0;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const int jl = slot_index(tx, c);
+            if (j0 + jl <= i) row[jl] = (vec ? Cs[rl * kGemmLd + jl] : crow[jl]) - acc[r][c];
+          }
         }
       }
     }
@@ -223,30 +304,26 @@ size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode) {
 
 int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
                   size_t ws_bytes, int32_t* info, cudaStream_t s) {
-  if ((mode & B2P_MODE_MASK) != B2P_MODE_FP32)
-    return set_error(B2P_ERR_UNSUPPORTED, "mode %d not available for n=%d", mode, n);
+  const int m = mode & B2P_MODE_MASK;
+  if (m == B2P_MODE_FP8 || (mode & B2P_FLAG_FP64_DIAG))
+    return set_error(B2P_ERR_UNSUPPORTED, "mode 0x%x not available for n=%d", mode, n);
+  const bool tensor = (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3);
   const size_t need = blocked_workspace_bytes(batch, n, mode);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
   float* tws = static_cast<float*>(ws);
   const int sms = device_sms();
-  {
-    const int64_t rows = batch * (int64_t)n;
-    const int grid = (int)std::min<int64_t>(rows, (int64_t)sms * 32);
-    {
-      TraceScope ts(kKCopyLower, s);
-      copy_lower_kernel<<<grid, 256, 0, s>>>(a, l, batch, n, info);
-    }
-    if (int st = check_launch("copy_lower_kernel")) return st;
-  }
-  const size_t dsmem = diag_smem_floats() * sizeof(float);
+  const size_t dsmem = sizeof(Diag64Smem);
   if (int st = ensure_smem_attr((const void*)diag_kernel, dsmem, kSlotDiag)) return st;
+  const size_t tsmem = (size_t)3 * kNB * kGemmLd * sizeof(float);
+  if (int st = ensure_smem_attr((const void*)trail_kernel, tsmem, kSlotTrail)) return st;
   const int gy = (int)std::min<int64_t>(batch, kMaxGridY);
   for (int k0 = 0; k0 < n; k0 += kNB) {
+    const float* src = (k0 == 0) ? a : l;
     const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
     {
       TraceScope ts(kKDiag, s);
-      diag_kernel<<<dgrid, kBlkThreads, dsmem, s>>>(l, batch, n, k0, tws, info);
+      diag_kernel<<<dgrid, kD64Threads, dsmem, s>>>(src, l, batch, n, k0, tws, info);
     }
     if (int st = check_launch("diag_kernel")) return st;
     const int R = n - k0 - kNB;
@@ -254,12 +331,16 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
     const int T = (R + kTile - 1) / kTile;
     {
       TraceScope ts(kKPanel, s);
-      panel_kernel<<<dim3(T, gy), kBlkThreads, 0, s>>>(l, batch, n, k0, tws);
+      panel_kernel<<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, batch, n, k0, tws);
     }
     if (int st = check_launch("panel_kernel")) return st;
+    if (tensor) {
+      if (int st = launch_syrk_tc(src, l, batch, n, k0, mode, info, s)) return st;
+      continue;
+    }
     {
       TraceScope ts(kKTrail, s);
-      trail_kernel<<<dim3(T * (T + 1) / 2, gy), kBlkThreads, 0, s>>>(l, batch, n, k0);
+      trail_kernel<<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, batch, n, k0);
     }
     if (int st = check_launch("trail_kernel")) return st;
   }

@@ -77,7 +77,9 @@ B2P_API size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode);
  *              (may be NULL when that size is 0), 256-byte aligned.
  *   info       optional device int32[batch]: 0 on success, k+1 when the
  *              k-th pivot was not positive (cuSOLVER potrf convention).  A
- *              non-SPD matrix yields NaN from the failing column on.
+ *              non-SPD matrix yields NaN from the failing column on.  -1
+ *              marks a matrix whose tensor-core update gave up a bounded
+ *              device-side wait (its output is then incomplete).
  *   stream     cudaStream_t (as void*).
  */
 B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mode,
@@ -128,6 +130,16 @@ B2P_API int b2p_potrf_ragged(const float* a, float* l, const int64_t* offsets_ho
 B2P_API size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n);
 B2P_API int b2p_potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch,
                        int64_t n, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Diagnostic: D[t] = A[t] * B[t]^T for `count` independent pairs of 128x64
+ * FP32 tiles (row-major, K contiguous) through the library's tcgen05 staging
+ * and MMA path; mode B2P_MODE_TF32 or B2P_MODE_BF16X3; err (device int32,
+ * optional) receives B2P_ERR_TIMEOUT if a bounded wait gave up.  Used to
+ * test the tensor-core path in isolation; no counterpart in the reference.
+ */
+B2P_API int b2p_debug_tc_gemm(const float* a, const float* b, float* d, int64_t count, int mode,
+                              int32_t* err, void* stream);
 
 /*
  * Launch trace: when enabled, every kernel the library launches is bracketed
