@@ -5,7 +5,18 @@ Drop-in for the GPU MODE ``cholesky`` entry point ``custom_kernel(A) -> L``
 behind a C ABI (``include/b200_potrf.h``), called from Python through ctypes.
 """
 
-from ._lib import PotrfError
+from ._lib import LaunchTrace, PotrfError
+from .autograd import CholeskyFunction, cholesky_differentiable, potrf_backward
+from .gp import gp_nll
 from .potrf import cholesky, custom_kernel
 
-__all__ = ["PotrfError", "cholesky", "custom_kernel"]
+__all__ = [
+    "CholeskyFunction",
+    "LaunchTrace",
+    "PotrfError",
+    "cholesky",
+    "cholesky_differentiable",
+    "custom_kernel",
+    "gp_nll",
+    "potrf_backward",
+]

@@ -4,7 +4,9 @@
 // custom_kernel (submission.py:4101-4268) by routing on n alone:
 //   n <= 32    one warp per matrix            (potrf_warp32_kernel)
 //   n <= 128   one CTA per matrix, in smem    (potrf_cta128_kernel)
-//   n >  128   blocked right-looking          (potrf_blocked)
+//   n >  128   tensor modes, n <= 1024, n % 64 == 0:
+//                fused left-looking, one CTA per matrix (potrf_fused)
+//              otherwise blocked right-looking  (potrf_blocked)
 // There is no CPU path and no vendor-library fallback.
 #include <cstdarg>
 #include <cstdio>
@@ -97,6 +99,7 @@ const char* b2p_last_error(void) { return g_msg; }
 
 size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode) {
   if (batch <= 0 || n <= 128) return 0;
+  if (fused_supported(n, mode)) return fused_workspace_bytes(batch, n);
   return blocked_workspace_bytes(batch, n, mode);
 }
 
@@ -116,7 +119,31 @@ int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mo
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
+  if (fused_supported(n, mode)) return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
   return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+}
+
+size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {
+  if (batch <= 0 || n <= 0) return 0;
+  return backward_workspace_bytes(batch, n);
+}
+
+int b2p_potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int64_t n, int mode,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+  g_msg[0] = '\0';
+  if (int st = check_mode(mode)) return st;
+  if (batch < 0 || n < 0 || n > (1 << 16))
+    return set_error(B2P_ERR_INVALID_ARG, "bad shape batch=%lld n=%lld", (long long)batch, (long long)n);
+  if (batch == 0 || n == 0) return B2P_OK;
+  if (l == nullptr || lbar == nullptr || abar == nullptr) return set_error(B2P_ERR_INVALID_ARG, "null pointer");
+  const size_t bytes = (size_t)batch * (size_t)n * (size_t)n * sizeof(float);
+  const char* pa = reinterpret_cast<const char*>(abar);
+  const char* pl = reinterpret_cast<const char*>(l);
+  const char* pg = reinterpret_cast<const char*>(lbar);
+  if ((pa < pl + bytes && pl < pa + bytes) || (pa < pg + bytes && pg < pa + bytes))
+    return set_error(B2P_ERR_INVALID_ARG, "abar overlaps l or lbar");
+  return potrf_backward(l, lbar, abar, batch, (int)n, mode, workspace, workspace_bytes,
+                        static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

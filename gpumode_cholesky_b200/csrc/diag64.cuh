@@ -105,13 +105,17 @@ __device__ __forceinline__ int diag64_factor_block(Diag64Smem& sm, int r0, float
 
 // Full 64x64 factor + inverse.  The caller has filled sm.S (lower triangle
 // and diagonal; identity padding beyond the true width) and synchronised.
-// Returns the first bad pivot (0..63) or -1, uniform across the CTA.
+// Returns the first bad pivot (0..63) or -1, uniform across the CTA.  Every
+// thread of the CTA must call it; threads beyond the first kD64Threads only
+// take part in the barriers.
 __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
+  const bool active = tid < kD64Threads;
   // T starts at zero (its upper-right block stays zero).
-  for (int e = tid; e < 64 * kD64Ld; e += kD64Threads) sm.T[e] = 0.0f;
+  if (active)
+    for (int e = tid; e < 64 * kD64Ld; e += kD64Threads) sm.T[e] = 0.0f;
   if (warp == 0) {
     const int b = diag64_factor_block(sm, 0, sm.lt0, sm.invd, lane);
     if (lane == 0) sm.bad[0] = b;
@@ -142,7 +146,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
     for (int j = 0; j < 32; ++j) sm.T[j * kD64Ld + lane] = y[j];
   }
   __syncthreads();
-  {
+  if (active) {
     // A22 -= L21 L21^T (lower part): thread -> row i, 8 columns.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
     float s[8];
@@ -178,7 +182,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
     col_inverse32(y, lane, sm.lt1, sm.invd + 32);
 #pragma unroll
     for (int j = 0; j < 32; ++j) sm.T[(32 + j) * kD64Ld + 32 + lane] = y[j];
-  } else if (warp >= 2) {
+  } else if (warp == 2 || warp == 3) {
     // W = L21 T11: thread -> row i, 16 columns; T11 rows are in sm.T.
     const int t = tid - 64;
     const int i = t >> 1, c0 = (t & 1) * 16;
@@ -202,7 +206,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
     for (int q = 0; q < 16; ++q) sm.w21[i * kLtLd + c0 + q] = s[q];
   }
   __syncthreads();
-  {
+  if (active) {
     // T21 = -T22 W: thread -> row i, 8 columns.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
     float s[8];
@@ -229,6 +233,73 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
   __syncthreads();
   const int b0 = sm.bad[0], b1 = sm.bad[1];
   return b0 >= 0 ? b0 : (b1 >= 0 ? 32 + b1 : -1);
+}
+
+// Inverse only: T = L^{-1} of the lower-triangular 64x64 block already in
+// sm.S (diagonal and lower part valid; identity padding beyond the true
+// width).  Uses lt0/lt1/p21t/w21 as scratch.  All threads call it.
+__device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const bool active = tid < kD64Threads;
+  if (active) {
+    for (int e = tid; e < 64 * kD64Ld; e += kD64Threads) sm.T[e] = 0.0f;
+    // L11^T, L22^T, L21^T and 1/diag.
+    for (int e = tid; e < 1024; e += kD64Threads) {
+      const int r = e >> 5, c = e & 31;
+      sm.lt0[c * kLtLd + r] = (c <= r) ? sm.S[r * kD64Ld + c] : 0.0f;
+      sm.lt1[c * kLtLd + r] = (c <= r) ? sm.S[(32 + r) * kD64Ld + 32 + c] : 0.0f;
+      sm.p21t[c * kLtLd + r] = sm.S[(32 + r) * kD64Ld + c];
+    }
+    if (tid < 64) sm.invd[tid] = 1.0f / sm.S[tid * kD64Ld + tid];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    float y[32];
+    col_inverse32(y, lane, sm.lt0, sm.invd);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sm.T[j * kD64Ld + lane] = y[j];
+  } else if (warp == 1) {
+    float y[32];
+    col_inverse32(y, lane, sm.lt1, sm.invd + 32);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) sm.T[(32 + j) * kD64Ld + 32 + lane] = y[j];
+  }
+  __syncthreads();
+  if (active) {
+    // W = L21 T11: thread -> row i, 8 columns.
+    const int i = tid >> 2, c0 = (tid & 3) * 8;
+    float sacc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sacc[q] = 0.0f;
+    for (int m = 0; m < 32; ++m) {
+      const float a = sm.p21t[m * kLtLd + i];
+      const float* trow = sm.T + m * kD64Ld + c0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sacc[q] = fmaf(a, trow[q], sacc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sm.w21[i * kLtLd + c0 + q] = sacc[q];
+  }
+  __syncthreads();
+  if (active) {
+    // T21 = -T22 W.
+    const int i = tid >> 2, c0 = (tid & 3) * 8;
+    float sacc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sacc[q] = 0.0f;
+    const float* trow = sm.T + (32 + i) * kD64Ld + 32;
+    for (int m = 0; m <= i; ++m) {
+      const float a = trow[m];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sacc[q] = fmaf(a, sm.w21[m * kLtLd + c0 + q], sacc[q]);
+    }
+    float* out = sm.T + (32 + i) * kD64Ld + c0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) out[q] = -sacc[q];
+  }
+  __syncthreads();
 }
 
 }  // namespace b2p

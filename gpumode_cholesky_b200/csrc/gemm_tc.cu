@@ -1,0 +1,248 @@
+// Batched GEMM on the tcgen05 tensor cores with structure hints, used by the
+// Cholesky adjoint (potrf_backward.cu).
+//
+//   C[b] = alpha * op1(X[b]) * op2(Y[b]) + beta * C[b]      (M x N, K inner)
+//
+// op1(X)[m][k] is X[m][k] (kTransNone) or X[k][m] (kTrans); op2(Y)[k][n] is
+// Y[k][n] or Y[n][k].  Structure hints let a 128x128 output tile skip the
+// parts of K where an operand is known to be zero (triangular operands), skip
+// tiles strictly above the diagonal when only the lower triangle of C is
+// wanted, and apply Phi (keep the lower triangle, halve the diagonal) in the
+// epilogue.  One 128-thread CTA per output tile: per 64-wide K chunk every
+// thread stages one operand row (128B-swizzled K-major, BF16 hi/lo split or
+// TF32), thread 0 issues the MMAs into a 128x128 FP32 TMEM accumulator, and
+// the epilogue reads TMEM with tcgen05.ld.  Waits are bounded.
+#include <algorithm>
+
+#include "launch.h"
+#include "umma.cuh"
+
+namespace b2p {
+
+constexpr int kGT = 128;  // tile edge
+constexpr int kGK = 64;   // K chunk
+constexpr int kGThreads = 128;
+constexpr uint32_t kGPolls = 1u << 24;
+constexpr size_t kGOperand = 32768;
+constexpr size_t kGSmem = 2 * kGOperand + 1024 + 64;
+
+
+__device__ __forceinline__ float g_round_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Write 64 K values of operand row r into the swizzled tile.
+template <int MODE>
+__device__ __forceinline__ void g_store_row(uint8_t* op, int r, const float (&v)[64]) {
+  if (MODE == B2P_MODE_TF32) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const float4 t = make_float4(g_round_tf32(v[4 * q]), g_round_tf32(v[4 * q + 1]), g_round_tf32(v[4 * q + 2]),
+                                   g_round_tf32(v[4 * q + 3]));
+      *reinterpret_cast<float4*>(op + (q >> 3) * 16384 + umma::sw128_offset(r, q & 7)) = t;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      uint32_t hi[4], lo[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        __nv_bfloat16 h0, l0, h1, l1;
+        umma::split_bf16(v[8 * c + 2 * p], h0, l0);
+        umma::split_bf16(v[8 * c + 2 * p + 1], h1, l1);
+        hi[p] = umma::pack_bf16(h0, h1);
+        lo[p] = umma::pack_bf16(l0, l1);
+      }
+      const uint32_t off = umma::sw128_offset(r, c);
+      *reinterpret_cast<uint4*>(op + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4*>(op + 16384 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+  }
+}
+
+// Operand row `r` (0..127) of a tile: logical element (row0 + r, k0 + kk).
+// `rowmajor`: element (i, kk) at mat[i*ld + kk] (K contiguous) else at
+// mat[kk*ld + i] (rows contiguous across threads: coalesced).
+template <int MODE>
+__device__ __forceinline__ void g_stage(const float* mat, int ld, bool rowmajor, int rows, int kdim, int row0,
+                                        int k0, uint8_t* op, int r) {
+  float v[64];
+  const int i = row0 + r;
+  if (rowmajor) {
+    const float* p = mat + (size_t)i * ld + k0;
+    const bool full = (i < rows) && (k0 + kGK <= kdim) && ((ld & 3) == 0);
+    if (full) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const float4 t = reinterpret_cast<const float4*>(p)[q];
+        v[4 * q] = t.x;
+        v[4 * q + 1] = t.y;
+        v[4 * q + 2] = t.z;
+        v[4 * q + 3] = t.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 64; ++q) v[q] = (i < rows && k0 + q < kdim) ? p[q] : 0.0f;
+    }
+  } else {
+    const float* p = mat + (size_t)k0 * ld + i;
+#pragma unroll
+    for (int q = 0; q < 64; ++q) v[q] = (i < rows && k0 + q < kdim) ? p[(size_t)q * ld] : 0.0f;
+  }
+  g_store_row<MODE>(op, r, v);
+}
+
+template <int MODE>
+__device__ __forceinline__ void g_mmas(uint32_t tmem, uint32_t a, uint32_t b, bool acc) {
+  if (MODE == B2P_MODE_TF32) {
+    constexpr uint32_t idesc = umma::idesc_f32acc(2, kGT, kGT);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const uint32_t off = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
+      umma::mma_tf32(tmem, umma::desc_k_sw128(a + off), umma::desc_k_sw128(b + off), idesc, (acc || s) ? 1u : 0u);
+    }
+  } else {
+    constexpr uint32_t idesc = umma::idesc_f32acc(1, kGT, kGT);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const uint32_t off = (uint32_t)(s * 32);
+      const uint64_t ah = umma::desc_k_sw128(a + off), al = umma::desc_k_sw128(a + 16384 + off);
+      const uint64_t bh = umma::desc_k_sw128(b + off), bl = umma::desc_k_sw128(b + 16384 + off);
+      umma::mma_bf16(tmem, al, bh, idesc, (acc || s) ? 1u : 0u);
+      umma::mma_bf16(tmem, ah, bl, idesc, 1u);
+      umma::mma_bf16(tmem, ah, bh, idesc, 1u);
+    }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(GemmArgs g, int tiles_n, int32_t* err) {
+  extern __shared__ unsigned char graw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(graw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* opA = base;
+  uint8_t* opB = base + kGOperand;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(base + 2 * kGOperand);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(base + 2 * kGOperand + 8);
+  int* flag = reinterpret_cast<int*>(base + 2 * kGOperand + 16);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // Tile coordinates (lower_out: triangular enumeration).
+  int tm, tn;
+  if (g.lower_out) {
+    const int q = blockIdx.x;
+    tm = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+    while ((tm + 1) * (tm + 2) / 2 <= q) ++tm;
+    while (tm * (tm + 1) / 2 > q) --tm;
+    tn = q - tm * (tm + 1) / 2;
+  } else {
+    tm = blockIdx.x / tiles_n;
+    tn = blockIdx.x - tm * tiles_n;
+  }
+  const int m0 = tm * kGT, n0 = tn * kGT;
+  // K range from the triangular hints.
+  int klo = 0, khi = g.k;
+  if (g.x_tri == 1) khi = min(khi, m0 + kGT);
+  if (g.x_tri == 2) klo = max(klo, m0);
+  if (g.y_tri == 1) klo = max(klo, n0);
+  if (g.y_tri == 2) khi = min(khi, n0 + kGT);
+  klo = (klo / kGK) * kGK;
+
+  if (tid == 0) *flag = 0;
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kGT);
+    umma::tmem_relinquish();
+  }
+  if (tid == 32) {
+    umma::mbar_init(mbar, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  uint32_t parity = 0;
+  bool ok = true;
+  int64_t b = blockIdx.y;
+  for (; b < g.batch && ok; b += gridDim.y) {
+    const float* X = g.x + b * g.sx;
+    const float* Y = g.y + b * g.sy;
+    float* C = g.c + b * g.sc;
+    bool any = false;
+    for (int k0 = klo; k0 < khi; k0 += kGK) {
+      // A operand: rows m (op1(X)[m][k]); B operand: rows n (op2(Y)[k][n]).
+      g_stage<MODE>(X, g.ldx, !g.trans_x, g.m, g.k, m0, k0, opA, tid);
+      g_stage<MODE>(Y, g.ldy, g.trans_y, g.n, g.k, n0, k0, opB, tid);
+      umma::fence_proxy_async_smem();
+      umma::fence_before_sync();
+      __syncthreads();
+      if (tid == 0) {
+        umma::fence_after_sync();
+        g_mmas<MODE>(tmem, umma::smem_u32(opA), umma::smem_u32(opB), any);
+        umma::mma_commit(mbar);
+      }
+      const bool got = umma::mbar_wait_bounded(mbar, parity, kGPolls);
+      parity ^= 1u;
+      umma::fence_after_sync();
+      if (!got) *flag = 1;
+      __syncthreads();
+      if (*flag) {
+        ok = false;
+        break;
+      }
+      any = true;
+    }
+    if (!ok) break;
+    // Epilogue: row i = m0 + 32*warp + lane, 4 chunks of 32 columns.
+    const int i = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int ch = 0; ch < 4; ++ch) {
+      float v[32];
+      if (any) {
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * ch), v);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) v[e] = 0.0f;
+      }
+      if (i < g.m) {
+        float* crow = C + (size_t)i * g.ldc;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          const int j = n0 + 32 * ch + e;
+          if (j < g.n && (!g.lower_out || j <= i)) {
+            float r = g.alpha * v[e];
+            if (g.phi) r = (j > i) ? 0.0f : (j == i ? 0.5f * r : r);
+            if (g.beta != 0.0f) r += g.beta * crow[j];
+            crow[j] = r;
+          }
+        }
+      }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  if (!ok && tid == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
+  if (!ok) umma::mbar_wait_bounded(mbar, parity ^ 1u, kGPolls);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kGT);
+}
+
+int launch_gemm_tc(const GemmArgs& g, int mode, int32_t* err, cudaStream_t s) {
+  if (g.batch <= 0 || g.m <= 0 || g.n <= 0) return B2P_OK;
+  const int tm = (g.m + kGT - 1) / kGT, tn = (g.n + kGT - 1) / kGT;
+  const int tiles = g.lower_out ? tm * (tm + 1) / 2 : tm * tn;
+  const dim3 grid(tiles, (unsigned)std::min<int64_t>(g.batch, 65535));
+  TraceScope ts(kKBwdGemm, s);
+  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
+    if (int st = ensure_smem_attr((const void*)gemm_tc_kernel<B2P_MODE_TF32>, kGSmem, kSlotBwd0)) return st;
+    gemm_tc_kernel<B2P_MODE_TF32><<<grid, kGThreads, kGSmem, s>>>(g, tn, err);
+  } else {
+    if (int st = ensure_smem_attr((const void*)gemm_tc_kernel<B2P_MODE_BF16X3>, kGSmem, kSlotBwd1)) return st;
+    gemm_tc_kernel<B2P_MODE_BF16X3><<<grid, kGThreads, kGSmem, s>>>(g, tn, err);
+  }
+  return check_launch("gemm_tc_kernel");
+}
+
+}  // namespace b2p

@@ -32,9 +32,33 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
 int launch_syrk_tc(const float* csrc, float* l, int64_t batch, int n, int k0, int mode, int32_t* info,
                    cudaStream_t s);
 
+// Fused left-looking tensor-core path for 128 < n <= 1024, n % 64 == 0 (potrf_fused.cu).
+bool fused_supported(int64_t n, int mode);
+size_t fused_workspace_bytes(int64_t batch, int64_t n);
+int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
+                int32_t* info, cudaStream_t s);
+
+// Batched tensor-core GEMM with structure hints (gemm_tc.cu):
+// C = alpha * op1(X) op2(Y) + beta * C per batch item.
+struct GemmArgs {
+  const float* x;
+  const float* y;
+  float* c;
+  int64_t sx, sy, sc;    // batch strides (elements)
+  int ldx, ldy, ldc;
+  int m, n, k;
+  int trans_x, trans_y;  // op1 = X^T / op2 = Y^T
+  int x_tri, y_tri;      // 0 none; 1: op(.) lower (op1: k <= m, op2: k >= n); 2: upper
+  int lower_out;         // write only C[i][j], j <= i (square M == N); skip tiles above
+  int phi;               // epilogue: zero above the diagonal, halve the diagonal
+  float alpha, beta;
+  int64_t batch;
+};
+int launch_gemm_tc(const GemmArgs& g, int mode, int32_t* err, cudaStream_t s);
+
 // Cholesky adjoint (potrf_backward.cu).
 size_t backward_workspace_bytes(int64_t batch, int64_t n);
-int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, void* ws,
+int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, int mode, void* ws,
                    size_t ws_bytes, cudaStream_t s);
 
 // Kernel ids reported by the launch trace (b2p_kernel_name).
@@ -52,6 +76,7 @@ enum KernelId {
   kKBwdGemm,
   kKBwdTrsm,
   kKBwdSym,
+  kKFused,
   kKCount
 };
 
@@ -80,6 +105,8 @@ enum SmemSlot {
   kSlotTc1,
   kSlotTc2,
   kSlotTc3,
+  kSlotFused0,
+  kSlotFused1,
   kSlotCount
 };
 

@@ -1,0 +1,173 @@
+// Cholesky adjoint: Abar = dLoss/dA from L and Lbar = dLoss/dL.
+//
+//   U  = L^{-1}                      block inverse: 64x64 diagonal blocks in
+//                                    shared memory, then a recursive
+//                                    U21 = -U22 (L21 U11) over block halves
+//   P  = Phi(tril(L^T Lbar))         lower triangle, diagonal halved
+//   Z  = P U                         lower x lower = lower
+//   S  = U^T Z                       ( = L^{-T} P L^{-1} )
+//   Abar = (S + S^T) / 2
+//
+// Every product runs on the tensor cores through gemm_tc.cu (BF16x3 or
+// TF32 operands, FP32 accumulation) with triangular K ranges.  The upper
+// part of Lbar is ignored: tril(L^T triu(Lbar, 1)) = 0.
+//
+// The reference has no backward; the oracle is torch.linalg.cholesky's
+// autograd (same formula) and FP64 finite differences.
+#include <algorithm>
+
+#include "diag64.cuh"
+#include "launch.h"
+
+namespace b2p {
+
+
+// Inverse of every 64x64 diagonal block of L into the same block of U.
+__global__ void __launch_bounds__(kD64Threads) trtri_diag_kernel(const float* __restrict__ l, float* __restrict__ u,
+                                                                 int64_t batch, int n) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  Diag64Smem& sm = *reinterpret_cast<Diag64Smem*>(raw);
+  const int tid = threadIdx.x;
+  const int k0 = blockIdx.x * 64;
+  const int w = min(64, n - k0);
+  for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
+    const size_t off = (size_t)b * n * n + (size_t)k0 * n + k0;
+    for (int e = tid; e < 4096; e += kD64Threads) {
+      const int r = e >> 6, c = e & 63;
+      float v = (r == c) ? 1.0f : 0.0f;
+      if (r < w && c < w) v = (c <= r) ? l[off + (size_t)r * n + c] : 0.0f;
+      sm.S[r * kD64Ld + c] = v;
+    }
+    __syncthreads();
+    diag64_invert_only(sm);
+    for (int e = tid; e < 4096; e += kD64Threads) {
+      const int r = e >> 6, c = e & 63;
+      if (r < w && c < w) u[off + (size_t)r * n + c] = sm.T[r * kD64Ld + c];
+    }
+    __syncthreads();
+  }
+}
+
+// out = (s + s^T) / 2, one element pair per thread.
+__global__ void sym_kernel(const float* __restrict__ s, float* __restrict__ out, int64_t batch, int n) {
+  const int64_t total = batch * (int64_t)n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = e / ((int64_t)n * n);
+    const int64_t r = e - b * (int64_t)n * n;
+    const int i = (int)(r / n), j = (int)(r - (int64_t)(r / n) * n);
+    const float* sb = s + b * (int64_t)n * n;
+    out[e] = 0.5f * (sb[(size_t)i * n + j] + sb[(size_t)j * n + i]);
+  }
+}
+
+static GemmArgs gemm_args(int64_t batch, int n) {
+  GemmArgs g{};
+  g.sx = g.sy = g.sc = (int64_t)n * n;
+  g.ldx = g.ldy = g.ldc = n;
+  g.alpha = 1.0f;
+  g.beta = 0.0f;
+  g.batch = batch;
+  return g;
+}
+
+// U[lo:hi, lo:hi] = inverse of L[lo:hi, lo:hi] (block indices, 64 wide);
+// diagonal blocks are already inverted.  tmp holds L21 U11.
+static int trtri_rec(const float* l, float* u, float* tmp, int64_t batch, int n, int lo, int hi, int mode,
+                     int32_t* err, cudaStream_t s) {
+  if (hi - lo <= 1) return B2P_OK;
+  const int mid = (lo + hi) / 2;
+  if (int st = trtri_rec(l, u, tmp, batch, n, lo, mid, mode, err, s)) return st;
+  if (int st = trtri_rec(l, u, tmp, batch, n, mid, hi, mode, err, s)) return st;
+  const int r0 = lo * 64, r1 = mid * 64, r2 = std::min(hi * 64, n);
+  const size_t o21 = (size_t)r1 * n + r0, o11 = (size_t)r0 * n + r0, o22 = (size_t)r1 * n + r1;
+  // tmp21 = L21 * U11   (U11 lower: op2(Y)[k][c] nonzero for k >= c)
+  GemmArgs g = gemm_args(batch, n);
+  g.x = l + o21;
+  g.y = u + o11;
+  g.c = tmp + o21;
+  g.m = r2 - r1;
+  g.n = r1 - r0;
+  g.k = r1 - r0;
+  g.y_tri = 1;
+  if (int st = launch_gemm_tc(g, mode, err, s)) return st;
+  // U21 = -U22 * tmp21   (U22 lower: op1(X)[m][k] nonzero for k <= m)
+  g = gemm_args(batch, n);
+  g.x = u + o22;
+  g.y = tmp + o21;
+  g.c = u + o21;
+  g.m = r2 - r1;
+  g.n = r1 - r0;
+  g.k = r2 - r1;
+  g.x_tri = 1;
+  g.alpha = -1.0f;
+  return launch_gemm_tc(g, mode, err, s);
+}
+
+size_t backward_workspace_bytes(int64_t batch, int64_t n) { return (size_t)2 * batch * n * n * sizeof(float); }
+
+int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, int mode, void* ws,
+                   size_t ws_bytes, cudaStream_t s) {
+  const int m = mode & B2P_MODE_MASK;
+  if (m != B2P_MODE_TF32 && m != B2P_MODE_BF16X3)
+    return set_error(B2P_ERR_UNSUPPORTED, "backward runs its products in tf32 or bf16x3 (mode 0x%x)", mode);
+  const size_t need = backward_workspace_bytes(batch, n);
+  if (ws == nullptr || ws_bytes < need)
+    return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
+  const size_t mat = (size_t)batch * n * n;
+  float* u = static_cast<float*>(ws);
+  float* w1 = u + mat;
+  int32_t* err = nullptr;
+  // U = L^{-1}: zero (upper part stays zero), diagonal blocks, recursion.
+  if (cudaMemsetAsync(u, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
+  const int nblk = (n + 63) / 64;
+  if (int st = ensure_smem_attr((const void*)trtri_diag_kernel, sizeof(Diag64Smem), kSlotBwd2)) return st;
+  {
+    TraceScope ts(kKBwdTrsm, s);
+    trtri_diag_kernel<<<dim3(nblk, (unsigned)std::min<int64_t>(batch, 65535)), kD64Threads, sizeof(Diag64Smem), s>>>(
+        l, u, batch, n);
+  }
+  if (int st = check_launch("trtri_diag_kernel")) return st;
+  if (int st = trtri_rec(l, u, w1, batch, n, 0, nblk, mode, err, s)) return st;
+  // P = Phi(tril(L^T Lbar)) into w1 (upper part zero).
+  if (cudaMemsetAsync(w1, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
+  GemmArgs g = gemm_args(batch, n);
+  g.x = l;
+  g.y = lbar;
+  g.c = w1;
+  g.m = g.n = g.k = n;
+  g.trans_x = 1;  // op1 = L^T: upper (k >= m)
+  g.x_tri = 2;
+  g.y_tri = 1;    // Lbar lower: k >= column
+  g.lower_out = 1;
+  g.phi = 1;
+  if (int st = launch_gemm_tc(g, mode, err, s)) return st;
+  // Z = P U into abar (lower; upper zero).
+  if (cudaMemsetAsync(abar, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
+  g = gemm_args(batch, n);
+  g.x = w1;
+  g.y = u;
+  g.c = abar;
+  g.m = g.n = g.k = n;
+  g.x_tri = 1;
+  g.y_tri = 1;
+  g.lower_out = 1;
+  if (int st = launch_gemm_tc(g, mode, err, s)) return st;
+  // S = U^T Z into w1.
+  g = gemm_args(batch, n);
+  g.x = u;
+  g.y = abar;
+  g.c = w1;
+  g.m = g.n = g.k = n;
+  g.trans_x = 1;
+  g.x_tri = 2;
+  g.y_tri = 1;
+  if (int st = launch_gemm_tc(g, mode, err, s)) return st;
+  {
+    TraceScope ts(kKBwdSym, s);
+    const int grid = (int)std::min<int64_t>((int64_t)((mat + 255) / 256), (int64_t)device_sms() * 32);
+    sym_kernel<<<grid, 256, 0, s>>>(w1, abar, batch, n);
+  }
+  return check_launch("sym_kernel");
+}
+
+}  // namespace b2p

@@ -17,10 +17,4 @@ int b2p_potrf_ragged(const float*, float*, const int64_t*, const int32_t*, const
   return set_error(B2P_ERR_UNSUPPORTED, "ragged batches are not built yet");
 }
 
-size_t b2p_potrf_backward_workspace_size(int64_t, int64_t) { return 0; }
-
-int b2p_potrf_backward(const float*, const float*, float*, int64_t, int64_t, void*, size_t, void*) {
-  return set_error(B2P_ERR_UNSUPPORTED, "backward is not built yet");
-}
-
 }  // extern "C"

@@ -118,6 +118,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
   return false;
 }
 
+// ---- bulk copies (untiled TMA, no multicast) -------------------------------
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+// Global -> shared copy of `bytes` (multiple of 16, both addresses 16-byte
+// aligned) completing as transaction bytes on `mbar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+      : "memory");
+}
+// Order generic-proxy writes (global and shared) before later async-proxy
+// accesses (bulk copies, tensor-core operand reads).
+__device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.proxy.async;" ::: "memory"); }
+
 // ---- TMEM -> registers -------------------------------------------------------
 // 32 lanes x 32 columns of 32-bit values: thread t of the warp receives lane
 // (lane_base + t), columns col..col+31.

@@ -124,12 +124,16 @@ B2P_API int b2p_potrf_ragged(const float* a, float* l, const int64_t* offsets_ho
  * (lower triangle used), writes Abar = dLoss/dA, symmetric:
  *   P = Phi(L^T Lbar)  (lower triangle, diagonal halved)
  *   Abar = 1/2 (S + S^T),  S = L^{-T} P L^{-1}.
+ * The products (L^{-1} by blocks, L^T Lbar, P L^{-1}, L^{-T} Z) run on the
+ * tensor cores; mode is B2P_MODE_BF16X3 (default accuracy, ~1e-6 relative)
+ * or B2P_MODE_TF32.  abar must not overlap l or lbar.
  * No counterpart exists in the reference (forward only); the oracle is
  * torch.linalg.cholesky's autograd and FP64 finite differences.
  */
 B2P_API size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n);
 B2P_API int b2p_potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch,
-                       int64_t n, void* workspace, size_t workspace_bytes, void* stream);
+                               int64_t n, int mode, void* workspace, size_t workspace_bytes,
+                               void* stream);
 
 /*
  * Diagnostic: D[t] = A[t] * B[t]^T for `count` independent pairs of 128x64
