@@ -42,11 +42,12 @@ SIGNATURES = {
     ),
     "b2p_noalloc_scratch_bytes": (_c_sz, []),
     "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),
-    "b2p_potrf_ragged_workspace_size": (_c_sz, [_c_p, _c_i64, ctypes.c_int]),
-    "b2p_potrf_ragged": (
-        ctypes.c_int,
-        [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
-    ),
+    "b2p_ragged_plan_create": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, ctypes.c_int, _c_p]),
+    "b2p_ragged_plan_destroy": (None, [_c_p]),
+    "b2p_ragged_plan_table_bytes": (_c_sz, [_c_p]),
+    "b2p_ragged_plan_workspace_bytes": (_c_sz, [_c_p]),
+    "b2p_ragged_plan_upload": (ctypes.c_int, [_c_p, _c_p, _c_p]),
+    "b2p_potrf_ragged": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_p, _c_p, _c_sz, _c_p, _c_p]),
     "b2p_potrf_backward_workspace_size": (_c_sz, [_c_i64, _c_i64]),
     "b2p_potrf_backward": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_sz, _c_p]),
     "b2p_debug_tc_gemm": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_p]),

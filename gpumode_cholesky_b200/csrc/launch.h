@@ -7,6 +7,7 @@
 
 #include "../../include/b200_potrf.h"
 #include "matrix_list.cuh"
+#include "sched.cuh"
 
 namespace b2p {
 
@@ -28,9 +29,13 @@ size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode);
 int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
                   size_t ws_bytes, int32_t* info, cudaStream_t s);
 
-// tcgen05 trailing update, TF32 or BF16x3 (syrk_tc.cu).
-int launch_syrk_tc(const float* csrc, float* l, int64_t batch, int n, int k0, int mode, int32_t* info,
-                   cudaStream_t s);
+// tcgen05 trailing update, TF32 or BF16x3 (syrk_tc.cu).  Dense: `tiles`
+// lower 128x128 tiles per matrix; ragged: one CTA per item of `sch`.
+int T_tc(int n, int k0);
+int launch_syrk_tc(const float* csrc, float* l, const Sched& sch, bool ragged, int tiles, int k0, int mode,
+                   int32_t* info, cudaStream_t s);
+int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const RaggedStep& st, int k0, int mode,
+                        float* tws, int32_t* info, cudaStream_t s);
 
 // Fused left-looking tensor-core path for 128 < n <= 1024, n % 64 == 0 (potrf_fused.cu).
 bool fused_supported(int64_t n, int mode);
@@ -107,6 +112,10 @@ enum SmemSlot {
   kSlotTc3,
   kSlotFused0,
   kSlotFused1,
+  kSlotDiagR,
+  kSlotTrailR,
+  kSlotTcR0,
+  kSlotTcR1,
   kSlotCount
 };
 

@@ -26,6 +26,7 @@
 
 #include "diag64.cuh"
 #include "launch.h"
+#include "sched.cuh"
 
 namespace b2p {
 
@@ -43,16 +44,20 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // -------------------------------------------------------------------------
 // diag: factor + invert the 64x64 diagonal block of every matrix.
+template <bool RAGGED>
 __global__ void __launch_bounds__(kD64Threads, 4)
-    diag_kernel(const float* __restrict__ src, float* __restrict__ l, int64_t batch, int n, int k0,
+    diag_kernel(const float* __restrict__ src, float* __restrict__ l, Sched sch, int k0,
                 float* __restrict__ tws, int32_t* __restrict__ info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Diag64Smem& sm = *reinterpret_cast<Diag64Smem*>(smem_raw);
   const int tid = threadIdx.x;
-  const int w = min(kNB, n - k0);
-  const bool vec = (n & 3) == 0;  // then w is a multiple of 4 as well
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
-    const size_t moff = (size_t)b * n * n + (size_t)k0 * n + k0;
+  for (int64_t it = blockIdx.x; it < sch.count; it += gridDim.x) {
+    const Target tg = resolve_matrix<RAGGED>(sch, it);
+    const int n = tg.n;
+    const int64_t b = tg.pos;
+    const int w = min(kNB, n - k0);
+    const bool vec = (n & 3) == 0;  // then w is a multiple of 4 as well
+    const size_t moff = tg.off + (size_t)k0 * n + k0;
     const float* in = src + moff;
     float* base = l + moff;
     if (vec) {
@@ -121,8 +126,8 @@ __global__ void __launch_bounds__(kD64Threads, 4)
       tb[e] = (m < w && c < w) ? sm.T[c * kD64Ld + m] : 0.0f;  // T^T[m][c] = T[c][m]
     }
     if (info != nullptr && tid == 0) {
-      if (k0 == 0) info[b] = bad >= 0 ? bad + 1 : 0;
-      else if (bad >= 0 && info[b] == 0) info[b] = k0 + bad + 1;
+      if (k0 == 0) info[tg.mat] = bad >= 0 ? bad + 1 : 0;
+      else if (bad >= 0 && info[tg.mat] == 0) info[tg.mat] = k0 + bad + 1;
     }
     __syncthreads();
   }
@@ -185,17 +190,22 @@ __device__ __forceinline__ void tile_mma_8x8(const float* As, const float* Bs, i
   }
 }
 
+template <bool RAGGED>
 __global__ void __launch_bounds__(kGemmThreads)
-    panel_kernel(const float* __restrict__ src, float* __restrict__ l, int64_t batch, int n, int k0,
+    panel_kernel(const float* __restrict__ src, float* __restrict__ l, Sched sch, int k0,
                  const float* __restrict__ tws) {
   __shared__ __align__(16) float Ps[kNB * kGemmLd];
   __shared__ __align__(16) float Ts[kNB * kGemmLd];
   const int tid = threadIdx.x;
   const int ty = tid >> 3, tx = tid & 7;
-  const int row0 = k0 + kNB + blockIdx.x * kTile;
-  for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
-    const size_t moff = (size_t)b * n * n;
-    const float* tb = tws + b * kNB * kNB;
+  const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
+  const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
+  for (int64_t it = start; it < sch.count; it += stride) {
+    const Target tg = resolve_tile<RAGGED>(sch, it);
+    const int n = tg.n;
+    const int row0 = k0 + kNB + tg.ti * kTile;
+    const size_t moff = tg.off;
+    const float* tb = tws + tg.pos * kNB * kNB;
 #pragma unroll
     for (int it = 0; it < 16; ++it) {
       const int e = tid + kGemmThreads * it;
@@ -230,24 +240,32 @@ __global__ void __launch_bounds__(kGemmThreads)
 // Trailing SYRK on lower 64x64 tiles.  The C tile is prefetched into shared
 // memory with cp.async while the panel tiles load and multiply; `csrc` is A
 // for the first block column and L afterwards, the result always goes to L.
+template <bool RAGGED>
 __global__ void __launch_bounds__(kGemmThreads)
-    trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, int64_t batch, int n, int k0) {
+    trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0) {
   extern __shared__ __align__(16) float tsm[];
   float* As = tsm;
   float* Bs = As + kNB * kGemmLd;
   float* Cs = Bs + kNB * kGemmLd;  // [64][kGemmLd], row-major C tile
   const int tid = threadIdx.x;
   const int ty = tid >> 3, tx = tid & 7;
-  const int q = blockIdx.x;
-  int ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
-  while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
-  while (ti * (ti + 1) / 2 > q) --ti;
-  const int tj = q - ti * (ti + 1) / 2;
-  const int t0 = k0 + kNB;
-  const int i0 = t0 + ti * kTile, j0 = t0 + tj * kTile;
-  const bool vec = (n & 3) == 0 && j0 + 64 <= n;
-  for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
-    const size_t moff = (size_t)b * n * n;
+  const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
+  const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
+  for (int64_t it = start; it < sch.count; it += stride) {
+    const Target tg = resolve_tile<RAGGED>(sch, it);
+    const int n = tg.n;
+    int ti = tg.ti, tj = tg.tj;
+    if (!RAGGED) {
+      const int q = blockIdx.x;
+      ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+      while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
+      while (ti * (ti + 1) / 2 > q) --ti;
+      tj = q - ti * (ti + 1) / 2;
+    }
+    const int t0 = k0 + kNB;
+    const int i0 = t0 + ti * kTile, j0 = t0 + tj * kTile;
+    const bool vec = (n & 3) == 0 && j0 + 64 <= n;
+    const size_t moff = tg.off;
     if (vec) {
 #pragma unroll
       for (int it = 0; it < 16; ++it) {
@@ -314,16 +332,17 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
   float* tws = static_cast<float*>(ws);
   const int sms = device_sms();
   const size_t dsmem = sizeof(Diag64Smem);
-  if (int st = ensure_smem_attr((const void*)diag_kernel, dsmem, kSlotDiag)) return st;
+  if (int st = ensure_smem_attr((const void*)diag_kernel<false>, dsmem, kSlotDiag)) return st;
   const size_t tsmem = (size_t)3 * kNB * kGemmLd * sizeof(float);
-  if (int st = ensure_smem_attr((const void*)trail_kernel, tsmem, kSlotTrail)) return st;
+  if (int st = ensure_smem_attr((const void*)trail_kernel<false>, tsmem, kSlotTrail)) return st;
   const int gy = (int)std::min<int64_t>(batch, kMaxGridY);
+  const Sched sch = dense_sched(batch, n);
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const float* src = (k0 == 0) ? a : l;
     const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
     {
       TraceScope ts(kKDiag, s);
-      diag_kernel<<<dgrid, kD64Threads, dsmem, s>>>(src, l, batch, n, k0, tws, info);
+      diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
     }
     if (int st = check_launch("diag_kernel")) return st;
     const int R = n - k0 - kNB;
@@ -331,20 +350,55 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
     const int T = (R + kTile - 1) / kTile;
     {
       TraceScope ts(kKPanel, s);
-      panel_kernel<<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, batch, n, k0, tws);
+      panel_kernel<false><<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, sch, k0, tws);
     }
     if (int st = check_launch("panel_kernel")) return st;
     if (tensor) {
-      if (int st = launch_syrk_tc(src, l, batch, n, k0, mode, info, s)) return st;
+      if (int st = launch_syrk_tc(src, l, sch, false, T_tc(n, k0), k0, mode, info, s)) return st;
       continue;
     }
     {
       TraceScope ts(kKTrail, s);
-      trail_kernel<<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, batch, n, k0);
+      trail_kernel<false><<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0);
     }
     if (int st = check_launch("trail_kernel")) return st;
   }
   return B2P_OK;
+}
+
+// One block-column step of the ragged schedule (potrf_ragged.cu builds it):
+// the first `ndiag` positions of the big-matrix list are active, `panel`
+// and `trail` are item lists on the device.
+int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const RaggedStep& st, int k0, int mode,
+                        float* tws, int32_t* info, cudaStream_t s) {
+  const int m = mode & B2P_MODE_MASK;
+  const bool tensor = (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3);
+  const float* src = (k0 == 0) ? a : l;
+  const int sms = device_sms();
+  const size_t dsmem = sizeof(Diag64Smem);
+  if (int e = ensure_smem_attr((const void*)diag_kernel<true>, dsmem, kSlotDiagR)) return e;
+  const size_t tsmem = (size_t)3 * kNB * kGemmLd * sizeof(float);
+  if (int e = ensure_smem_attr((const void*)trail_kernel<true>, tsmem, kSlotTrailR)) return e;
+  Sched sd = ragged_sched(t, nullptr, st.ndiag);
+  if (st.ndiag > 0) {
+    TraceScope ts(kKDiag, s);
+    diag_kernel<true><<<(int)std::min<int64_t>(st.ndiag, (int64_t)sms * 16), kD64Threads, dsmem, s>>>(
+        src, l, sd, k0, tws, info);
+  }
+  if (int e = check_launch("diag_kernel<ragged>")) return e;
+  if (st.npanel > 0) {
+    Sched sp = ragged_sched(t, t.items + st.panel_beg, st.npanel);
+    TraceScope ts(kKPanel, s);
+    panel_kernel<true><<<(int)std::min<int64_t>(st.npanel, 1 << 30), kGemmThreads, 0, s>>>(src, l, sp, k0, tws);
+  }
+  if (int e = check_launch("panel_kernel<ragged>")) return e;
+  if (st.ntrail > 0) {
+    Sched sr = ragged_sched(t, t.items + st.trail_beg, st.ntrail);
+    if (tensor) return launch_syrk_tc(src, l, sr, true, 0, k0, mode, info, s);
+    TraceScope ts(kKTrail, s);
+    trail_kernel<true><<<(int)std::min<int64_t>(st.ntrail, 1 << 30), kGemmThreads, tsmem, s>>>(src, l, sr, k0);
+  }
+  return check_launch("trail_kernel<ragged>");
 }
 
 }  // namespace b2p

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "launch.h"
+#include "sched.cuh"
 #include "umma.cuh"
 
 namespace b2p {
@@ -171,9 +172,9 @@ __device__ __forceinline__ void tc_teardown(const TcShared& sh, uint32_t tmem, b
   if ((threadIdx.x >> 5) == 0) umma::tmem_dealloc(tmem, kTcTile);
 }
 
-template <int MODE>
+template <int MODE, bool RAGGED>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    syrk_tc_kernel(const float* __restrict__ csrc, float* __restrict__ l, int64_t batch, int n, int k0,
+    syrk_tc_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0,
                    int32_t* __restrict__ info) {
   extern __shared__ unsigned char tc_raw[];
   const TcShared sh = tc_layout(tc_raw);
@@ -181,19 +182,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (tid == 0) *sh.flag = 0;
   tc_setup(sh);
   const uint32_t tmem = *sh.tslot;
-  const int q = blockIdx.x;
-  int ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
-  while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
-  while (ti * (ti + 1) / 2 > q) --ti;
-  const int tj = q - ti * (ti + 1) / 2;
-  const int t0 = k0 + kTcK;
-  const int i0 = t0 + ti * kTcTile, j0 = t0 + tj * kTcTile;
-  const bool vec = (n & 3) == 0;
   uint32_t parity = 0;
   bool ok = true;
-  int64_t b = blockIdx.y;
-  for (; b < batch && ok; b += gridDim.y) {
-    const size_t moff = (size_t)b * n * n;
+  const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
+  const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
+  int64_t it = start;
+  int64_t cur_mat = -1;
+  for (; it < sch.count && ok; it += stride) {
+    const Target tg = resolve_tile<RAGGED>(sch, it);
+    cur_mat = tg.mat;
+    const int n = tg.n;
+    int ti = tg.ti, tj = tg.tj;
+    if (!RAGGED) {
+      const int q = blockIdx.x;
+      ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+      while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
+      while (ti * (ti + 1) / 2 > q) --ti;
+      tj = q - ti * (ti + 1) / 2;
+    }
+    const int t0 = k0 + kTcK;
+    const int i0 = t0 + ti * kTcTile, j0 = t0 + tj * kTcTile;
+    const bool vec = (n & 3) == 0;
+    const size_t moff = tg.off;
     const float* mat = l + moff;
     {
       const int ia = i0 + tid;
@@ -237,7 +247,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
   }
   // A timed-out wait marks the matrix it was working on with info = -1.
-  if (!ok && tid == 0 && info != nullptr && b < batch) info[b] = -1;
+  if (!ok && tid == 0 && info != nullptr && cur_mat >= 0) info[cur_mat] = -1;
   tc_teardown(sh, tmem, ok, parity);
 }
 
@@ -276,20 +286,40 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   tc_teardown(sh, tmem, ok, parity);
 }
 
-int launch_syrk_tc(const float* csrc, float* l, int64_t batch, int n, int k0, int mode, int32_t* info,
-                   cudaStream_t s) {
+int T_tc(int n, int k0) {
   const int R = n - k0 - kTcK;
-  if (R <= 0) return B2P_OK;
-  const int T = (R + kTcTile - 1) / kTcTile;
-  const int gy = (int)std::min<int64_t>(batch, 65535);
-  const dim3 grid(T * (T + 1) / 2, gy);
-  TraceScope ts(kKTrailTc, s);
-  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
-    if (int st = ensure_smem_attr((const void*)syrk_tc_kernel<B2P_MODE_TF32>, kTcSmemBytes, kSlotTc0)) return st;
-    syrk_tc_kernel<B2P_MODE_TF32><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, batch, n, k0, info);
+  return R <= 0 ? 0 : (R + kTcTile - 1) / kTcTile;
+}
+
+int launch_syrk_tc(const float* csrc, float* l, const Sched& sch, bool ragged, int tiles, int k0, int mode,
+                   int32_t* info, cudaStream_t s) {
+  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
+  const void* fn;
+  int slot;
+  if (ragged) {
+    fn = tf32 ? (const void*)syrk_tc_kernel<B2P_MODE_TF32, true> : (const void*)syrk_tc_kernel<B2P_MODE_BF16X3, true>;
+    slot = tf32 ? kSlotTcR0 : kSlotTcR1;
   } else {
-    if (int st = ensure_smem_attr((const void*)syrk_tc_kernel<B2P_MODE_BF16X3>, kTcSmemBytes, kSlotTc1)) return st;
-    syrk_tc_kernel<B2P_MODE_BF16X3><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, batch, n, k0, info);
+    fn = tf32 ? (const void*)syrk_tc_kernel<B2P_MODE_TF32, false>
+              : (const void*)syrk_tc_kernel<B2P_MODE_BF16X3, false>;
+    slot = tf32 ? kSlotTc0 : kSlotTc1;
+  }
+  if (int st = ensure_smem_attr(fn, kTcSmemBytes, slot)) return st;
+  dim3 grid;
+  if (ragged) {
+    if (sch.count <= 0) return B2P_OK;
+    grid = dim3((unsigned)std::min<int64_t>(sch.count, 1 << 30), 1);
+  } else {
+    if (tiles <= 0 || sch.count <= 0) return B2P_OK;
+    grid = dim3(tiles * (tiles + 1) / 2, (unsigned)std::min<int64_t>(sch.count, 65535));
+  }
+  TraceScope ts(kKTrailTc, s);
+  if (ragged) {
+    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
+    else syrk_tc_kernel<B2P_MODE_BF16X3, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
+  } else {
+    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
+    else syrk_tc_kernel<B2P_MODE_BF16X3, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
   }
   return check_launch("syrk_tc_kernel");
 }

@@ -1,0 +1,135 @@
+"""Ragged batches: many SPD matrices of different orders in one packed buffer.
+
+A :class:`RaggedPlan` is built once per list of orders (host-side schedule
+in the library, tables uploaded to the device once); :meth:`RaggedPlan.factor`
+then enqueues the whole factorization on the current stream without host
+synchronisation, and :meth:`RaggedPlan.capture` records it into a CUDA graph
+that replays the entire ragged batch as one graph launch.
+
+Layout: matrix i occupies ``buf[offsets[i] : offsets[i] + n_i * n_i]``
+(row-major), offsets multiples of 4 elements (16 bytes).  The reference has
+no ragged path (its dispatcher routes exact (batch, n) shapes only,
+submission.py:4111-4268).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from collections.abc import Sequence
+
+import torch
+
+from . import _lib
+from .inputs import pack_offsets
+from .potrf import _stream_ptr, resolve_mode
+
+
+def pack(mats: Sequence[torch.Tensor], device=None) -> tuple[torch.Tensor, list[int], list[int]]:
+    """Pack square FP32 matrices into one buffer; returns (buffer, orders, offsets)."""
+    orders = [int(m.shape[-1]) for m in mats]
+    offs = pack_offsets(orders)
+    dev = device if device is not None else (mats[0].device if mats else "cpu")
+    buf = torch.zeros(offs[-1], dtype=torch.float32, device=dev)
+    for m, n, o in zip(mats, orders, offs):
+        buf[o : o + n * n] = m.reshape(-1).to(device=dev, dtype=torch.float32)
+    return buf, orders, offs[:-1]
+
+
+def unpack(buf: torch.Tensor, orders: Sequence[int], offsets: Sequence[int]) -> list[torch.Tensor]:
+    """Views of the packed matrices."""
+    return [buf[o : o + n * n].view(n, n) for n, o in zip(orders, offsets)]
+
+
+class RaggedPlan:
+    """Schedule for one list of orders (and offsets) on one device."""
+
+    def __init__(
+        self,
+        orders: Sequence[int],
+        offsets: Sequence[int] | None = None,
+        mode: str | int | None = None,
+        tc_min_n: int = 0,
+        device: torch.device | str | None = None,
+    ):
+        self.orders = [int(n) for n in orders]
+        self.offsets = [int(o) for o in (offsets if offsets is not None else pack_offsets(self.orders)[:-1])]
+        if len(self.offsets) != len(self.orders):
+            raise ValueError("orders and offsets differ in length")
+        self.count = len(self.orders)
+        self.total = max((o + n * n for n, o in zip(self.orders, self.offsets)), default=0)
+        self.mode = resolve_mode(mode, max(self.orders, default=0))
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        lib = _lib.load()
+        offs = (ctypes.c_int64 * max(self.count, 1))(*self.offsets)
+        ns = (ctypes.c_int32 * max(self.count, 1))(*self.orders)
+        handle = ctypes.c_void_p()
+        _lib.check(
+            lib.b2p_ragged_plan_create(offs, ns, self.count, self.mode, int(tc_min_n), ctypes.byref(handle)),
+            "b2p_ragged_plan_create",
+        )
+        self._handle = handle
+        self.table_bytes = lib.b2p_ragged_plan_table_bytes(handle)
+        self.workspace_bytes = lib.b2p_ragged_plan_workspace_bytes(handle)
+        self.tables = torch.empty(max(self.table_bytes, 16), dtype=torch.uint8, device=self.device)
+        self.workspace = torch.empty(max(self.workspace_bytes, 256), dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                lib.b2p_ragged_plan_upload(handle, self.tables.data_ptr(), _stream_ptr(self.device)),
+                "b2p_ragged_plan_upload",
+            )
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None) is not None and self._handle.value:
+            _lib.load().b2p_ragged_plan_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def factor(self, a: torch.Tensor, out: torch.Tensor | None = None, info: torch.Tensor | None = None):
+        """Factor every matrix of the packed buffer ``a`` into ``out`` (same layout)."""
+        if not a.is_cuda or a.dtype != torch.float32 or a.dim() != 1:
+            raise ValueError("a must be a 1-D float32 CUDA buffer")
+        if a.numel() < self.total:
+            raise ValueError(f"buffer holds {a.numel()} elements, the plan needs {self.total}")
+        if out is None:
+            out = torch.empty_like(a)
+        if info is not None and (info.dtype != torch.int32 or info.numel() < self.count):
+            raise ValueError("info must be int32 with one entry per matrix")
+        with torch.cuda.device(a.device):
+            st = _lib.load().b2p_potrf_ragged(
+                self._handle,
+                self.tables.data_ptr(),
+                a.data_ptr(),
+                out.data_ptr(),
+                self.workspace.data_ptr(),
+                self.workspace.numel(),
+                info.data_ptr() if info is not None else None,
+                _stream_ptr(a.device),
+            )
+        _lib.check(st, "b2p_potrf_ragged")
+        return out
+
+    def capture(self, a_static: torch.Tensor, out_static: torch.Tensor) -> torch.cuda.CUDAGraph:
+        """Record factor(a_static -> out_static) into a CUDA graph (replay with ``g.replay()``)."""
+        self.factor(a_static, out_static)  # warm: sets kernel attributes outside capture
+        torch.cuda.synchronize(a_static.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.factor(a_static, out_static)
+        return g
+
+
+def cholesky_ragged(
+    a: torch.Tensor, orders: Sequence[int], offsets: Sequence[int] | None = None, mode: str | int | None = None
+) -> torch.Tensor:
+    """One-shot ragged factorization (builds a plan each call)."""
+    plan = RaggedPlan(orders, offsets, mode=mode, device=a.device)
+    try:
+        return plan.factor(a)
+    finally:
+        torch.cuda.current_stream(a.device).synchronize()
+        plan.close()

@@ -105,19 +105,32 @@ B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, i
                                       int mode, int32_t* info, void* stream);
 
 /*
- * Ragged batch: `count` matrices of individual order n_host[i] packed in one
- * buffer, matrix i starting at element offsets_host[i] (each row-major,
- * contiguous, n_i*n_i floats, offsets multiples of 4).  The host arrays are
- * read during the call only to size the schedule; the device copies
- * (offsets_dev, n_dev, same contents) are what the kernels read, so the call
- * can be replayed from a CUDA graph.  No counterpart exists in the reference
- * (its dispatcher routes exact (batch, n) shapes only, submission.py:4111-4268).
+ * Ragged batches: `count` matrices of individual order n_host[i] packed in
+ * one buffer, matrix i starting at element offsets_host[i] (row-major,
+ * contiguous n_i*n_i floats; offsets multiples of 4).  The output buffer uses
+ * the same offsets.  Usage:
+ *   b2p_ragged_plan_create   host-only: buckets the orders and precomputes
+ *                            every launch (tc_min_n: in tensor modes, the
+ *                            smallest order whose trailing updates use the
+ *                            tensor cores; 0 = default 256);
+ *   b2p_ragged_plan_upload   copies the plan's tables (table_bytes, 16-byte
+ *                            aligned device buffer) to the device; blocking;
+ *   b2p_potrf_ragged         enqueues the factorization; reads only device
+ *                            memory, so it can be captured in a CUDA graph;
+ *   b2p_ragged_plan_destroy.
+ * info (optional, device int32[count]) follows b2p_potrf_batched.  No
+ * counterpart exists in the reference (its dispatcher routes exact
+ * (batch, n) shapes only, submission.py:4111-4268).
  */
-B2P_API size_t b2p_potrf_ragged_workspace_size(const int32_t* n_host, int64_t count, int mode);
-B2P_API int b2p_potrf_ragged(const float* a, float* l, const int64_t* offsets_host,
-                     const int32_t* n_host, const int64_t* offsets_dev,
-                     const int32_t* n_dev, int64_t count, int mode, void* workspace,
-                     size_t workspace_bytes, int32_t* info, void* stream);
+typedef struct b2p_ragged_plan b2p_ragged_plan;
+B2P_API int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, int64_t count,
+                                   int mode, int tc_min_n, b2p_ragged_plan** plan);
+B2P_API void b2p_ragged_plan_destroy(b2p_ragged_plan* plan);
+B2P_API size_t b2p_ragged_plan_table_bytes(const b2p_ragged_plan* plan);
+B2P_API size_t b2p_ragged_plan_workspace_bytes(const b2p_ragged_plan* plan);
+B2P_API int b2p_ragged_plan_upload(const b2p_ragged_plan* plan, void* tables, void* stream);
+B2P_API int b2p_potrf_ragged(const b2p_ragged_plan* plan, const void* tables, const float* a, float* l,
+                             void* workspace, size_t workspace_bytes, int32_t* info, void* stream);
 
 /*
  * Cholesky adjoint: given L (output of the factorization) and Lbar = dLoss/dL

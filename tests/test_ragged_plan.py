@@ -1,0 +1,63 @@
+"""CPU: the ragged plan is host-only and validates its input."""
+
+from __future__ import annotations
+
+import ctypes
+
+from gpumode_cholesky_b200 import _lib, inputs
+
+
+def _plan(orders, offsets=None, mode=0, tc_min_n=0):
+    lib = _lib.load()
+    offsets = offsets if offsets is not None else inputs.pack_offsets(orders)[:-1]
+    offs = (ctypes.c_int64 * max(len(orders), 1))(*offsets)
+    ns = (ctypes.c_int32 * max(len(orders), 1))(*orders)
+    h = ctypes.c_void_p()
+    st = lib.b2p_ragged_plan_create(offs, ns, len(orders), mode, tc_min_n, ctypes.byref(h))
+    return st, h
+
+
+def test_plan_sizes_and_destroy():
+    lib = _lib.load()
+    orders = [1, 16, 32, 33, 100, 128, 129, 300, 1000]
+    st, h = _plan(orders)
+    assert st == _lib.B2P_OK
+    # three big matrices -> one 64x64 inverse slot each
+    assert lib.b2p_ragged_plan_workspace_bytes(h) == 3 * 64 * 64 * 4
+    assert lib.b2p_ragged_plan_table_bytes(h) > 8 * len(orders)
+    lib.b2p_ragged_plan_destroy(h)
+
+
+def test_plan_empty_and_small_only():
+    lib = _lib.load()
+    st, h = _plan([])
+    assert st == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) == 0
+    lib.b2p_ragged_plan_destroy(h)
+    st, h = _plan([3, 7, 32, 64, 128])
+    assert st == _lib.B2P_OK and lib.b2p_ragged_plan_workspace_bytes(h) == 0
+    lib.b2p_ragged_plan_destroy(h)
+
+
+def test_plan_rejects_bad_input():
+    lib = _lib.load()
+    st, h = _plan([8, 8], offsets=[0, 66])  # not a multiple of 4
+    assert st == _lib.B2P_ERR_INVALID_ARG and not h.value
+    assert b"multiples of 4" in lib.b2p_last_error()
+    st, h = _plan([8, -1])
+    assert st == _lib.B2P_ERR_INVALID_ARG
+    st, h = _plan([8], mode=_lib.MODE_FP8)
+    assert st == _lib.B2P_ERR_UNSUPPORTED
+
+
+def test_config4_orders_plan():
+    """The 3000-matrix log-uniform [16, 2048] draw plans without a device."""
+    lib = _lib.load()
+    orders = inputs.ragged_orders(3000, seed=4)
+    assert min(orders) >= 16 and max(orders) <= 2048
+    for mode in (0, _lib.MODE_BF16X3):
+        st, h = _plan(orders, mode=mode)
+        assert st == _lib.B2P_OK
+        big = sum(1 for n in orders if n > 128)
+        assert lib.b2p_ragged_plan_workspace_bytes(h) == big * 64 * 64 * 4
+        lib.b2p_ragged_plan_destroy(h)
