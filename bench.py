@@ -1,25 +1,34 @@
 #!/usr/bin/env python
 """Benchmark of the batched Cholesky hot path on B200.
 
-Workload (one "step"): factor the two plain-FP32 mid-size batches of the
-benchmark suite, 640 matrices of order 512 and 60 of order 1024, each batch
-half well-conditioned (M M^T/n + I) and half prescribed-spectrum
-(Q diag(logspace[1, 1e6]) Q^T).  Inputs are synthetic and seeded, resident
-in HBM (0.92 GB, larger than the 126 MB L2, so no flush is needed between
-steps).  ``value`` is device time per step in microseconds (lower is better).
+Default workload ("mid", one "step"): factor the two plain-FP32 mid-size
+batches of the benchmark suite, 640 matrices of order 512 and 60 of order
+1024, each batch half well-conditioned (M M^T/n + I) and half
+prescribed-spectrum (Q diag(logspace[1, 1e6]) Q^T).  Inputs are synthetic,
+seeded and resident in HBM (0.92 GB, larger than the 126 MB L2, so no flush
+is needed between steps).  ``value`` is device time per step in microseconds
+(lower is better) in the chosen precision mode ("auto" = BF16x3 trailing
+updates for n > 128, the mixed form that meets the 1e-5 relative residual);
+the plain FP32 form and cuSOLVER on the same GPU are reported beside it.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp32|bf16x3|tf32|auto]
+Other workloads (profiling and extra lines, not the headline):
+  small   4096 x 32 (HBM-bound; 8 rotating input sets, 256 MiB > L2)
+  large   1 x 8192 (GG^T/n + 0.1 I)
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode auto|fp32|bf16x3|tf32]
     python bench.py --impl reference     # the reference's CPU route, timed on host cores
 
 With N > 1 (torchrun) every rank factors its own full step (weak scaling, no
 collective on the data path); the reported time is the max over ranks.
+Steps are replayed from a CUDA graph captured once (launch overhead is not
+part of the device time); ``e2e`` instead calls the public entry point per
+step with host<->device copies.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -33,10 +42,32 @@ if str(ROOT) not in sys.path:
 
 import torch  # noqa: E402
 
-SHAPES = [(640, 512), (60, 1024)]
-SEEDS = {512: 510512, 1024: 511024}
-WORKLOAD = "mid-size batched potrf: 640x512 + 60x1024 FP32, half MM^T/n+I, half spectrum [1,1e6]"
-METRIC = "batched potrf us per step (640x512 + 60x1024)"
+WORKLOADS = {
+    "mid": {
+        "shapes": [(640, 512), (60, 1024)],
+        "seeds": [510512, 511024],
+        "gen": "mixed",
+        "sets": 1,
+        "desc": "mid-size batched potrf: 640x512 + 60x1024 FP32, half MM^T/n+I, half spectrum [1,1e6]",
+        "metric": "batched potrf us per step (640x512 + 60x1024)",
+    },
+    "small": {
+        "shapes": [(4096, 32)],
+        "seeds": [41032],
+        "gen": "well",
+        "sets": 8,
+        "desc": "small batched potrf: 4096x32 FP32, MM^T/n+I",
+        "metric": "batched potrf us per step (4096x32)",
+    },
+    "large": {
+        "shapes": [(1, 8192)],
+        "seeds": [48192],
+        "gen": "gram",
+        "sets": 1,
+        "desc": "large potrf: 1x8192 FP32, GG^T/n+0.1I",
+        "metric": "potrf us per step (1x8192)",
+    },
+}
 
 
 def _dist():
@@ -48,6 +79,16 @@ def _dist():
 
 def _flops(batch: int, n: int) -> float:
     return batch * n**3 / 3.0
+
+
+def _make(gen: str, b: int, n: int, seed: int, device):
+    from gpumode_cholesky_b200 import inputs
+
+    if gen == "mixed":
+        return inputs.mixed_batch(b, n, seed, device=device)
+    if gen == "gram":
+        return inputs.large_gram(n, seed, device=device).expand(b, n, n).contiguous()
+    return inputs.well_conditioned(b, n, seed, device=device)
 
 
 def _clock_sampler_start(gpu_index: int):
@@ -113,21 +154,29 @@ def _measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "src": "measured"}
-    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "fallback"}
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "src": "of measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "src": "of fallback"}
 
 
 def _profiled_traffic() -> dict:
-    """DRAM bytes per launch of the dominant kernels from the committed ncu summaries."""
+    """DRAM bytes per algorithmic byte (or flop) of a kernel, from the committed ncu summaries.
+
+    A summary line reads ``traffic_per_unit: <kernel> <workload> <mode> <value>``.
+    """
     out = {}
     for p in (ROOT / "profiles").glob("*.md"):
         for line in p.read_text().splitlines():
-            if line.startswith("traffic_bytes_per_unit:"):
-                # traffic_bytes_per_unit: <kernel> <mode> <bytes per algorithmic byte/flop>
+            if line.startswith("traffic_per_unit:"):
                 parts = line.split()
-                if len(parts) >= 4:
-                    out[(parts[1], parts[2])] = float(parts[3])
+                if len(parts) >= 5:
+                    out[(parts[1], parts[2], parts[3])] = float(parts[4])
     return out
+
+
+def _resolve_mode(mode: str, n: int):
+    if mode != "auto":
+        return mode
+    return "bf16x3" if n > 128 else "fp32"
 
 
 # ---------------------------------------------------------------------------
@@ -137,13 +186,12 @@ def run_reference(args) -> int:
     if rank != 0:
         return 0
     import oracle  # the CPU leg may use the oracle package (reference route restated there)
-    from gpumode_cholesky_b200 import inputs
 
+    wl = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    frac = args.ref_sample
-    sample = [(max(1, int(round(b * frac))), n) for b, n in SHAPES]
-    data = [inputs.mixed_batch(b, n, SEEDS[n], device="cpu") for b, n in sample]
+    sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+    data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for _ in range(args.warmup):
         for a in data:
             oracle.ref_kernel_cpu(a)
@@ -152,12 +200,12 @@ def run_reference(args) -> int:
         for a in data:
             oracle.ref_kernel_cpu(a)
     dt = (time.perf_counter() - t0) / args.steps
-    scale = sum(_flops(b, n) for b, n in SHAPES) / sum(_flops(b, n) for b, n in sample)
+    scale = sum(_flops(b, n) for b, n in wl["shapes"]) / sum(_flops(b, n) for b, n in sample)
     us = dt * 1e6 * scale
     desc = " + ".join(f"{b}x{n}" for b, n in sample) + f" per step, scaled by flops x{scale:.2f} to the full step"
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": wl["metric"],
         "value": round(us, 1),
         "unit": "us",
         "n_gpus": ws,
@@ -169,7 +217,7 @@ def run_reference(args) -> int:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "inputs larger than L2"},
+        "config": {"workload": wl["desc"], "l2": "inputs larger than L2"},
         "cpu_baseline": {
             "value": round(us, 1),
             "unit": "us",
@@ -184,6 +232,18 @@ def run_reference(args) -> int:
 
 
 # ---------------------------------------------------------------------------
+def _timed(fn, k: int) -> float:
+    """Mean ms per call of k calls, CUDA events on the current stream."""
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(k):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / k
+
+
 def run_ours(args) -> int:
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
@@ -194,30 +254,42 @@ def run_ours(args) -> int:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    from gpumode_cholesky_b200 import _lib, build, inputs
+    from gpumode_cholesky_b200 import _lib, build
     from gpumode_cholesky_b200.potrf import cholesky
 
     if not build.LIB_PATH.exists():
         build.build()
     _lib.load()
-    mode = args.mode
-    data = [inputs.mixed_batch(b, n, SEEDS[n] + 7919 * rank, device=dev) for b, n in SHAPES]
-    outs = [torch.empty_like(a) for a in data]
+    wl = WORKLOADS[args.workload]
+    shapes = [(max(1, int(round(b * args.scale))), n) for b, n in wl["shapes"]]
+    modes = [_resolve_mode(args.mode, n) for _, n in shapes]
+    sets = [
+        [_make(wl["gen"], b, n, s + 7919 * rank + 104729 * k, dev) for (b, n), s in zip(shapes, wl["seeds"])]
+        for k in range(wl["sets"])
+    ]
+    outs = [[torch.empty_like(a) for a in st] for st in sets]
     torch.cuda.synchronize()
 
-    def step(m):
-        for a, o in zip(data, outs):
+    def eager_step(i: int, mode_list=None):
+        ml = mode_list or modes
+        for a, o, m in zip(sets[i % len(sets)], outs[i % len(sets)], ml):
             cholesky(a, mode=m, out=o)
 
-    def timed(fn, k):
-        s = torch.cuda.current_stream()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        for _ in range(k):
-            fn()
-        e1.record(s)
-        e1.synchronize()
-        return e0.elapsed_time(e1) / k
+    # One CUDA graph per input set (warm-up first: kernel attributes are set outside capture).
+    for i in range(len(sets)):
+        eager_step(i)
+    torch.cuda.synchronize()
+    graphs = []
+    for i in range(len(sets)):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            eager_step(i)
+        graphs.append(g)
+    counter = [0]
+
+    def step():
+        graphs[counter[0] % len(graphs)].replay()
+        counter[0] += 1
 
     def barrier():
         if ws > 1:
@@ -228,11 +300,11 @@ def run_ours(args) -> int:
     clk = _clock_sampler_start(local)
     time.sleep(0.3)  # let nvidia-smi start sampling
     for _ in range(args.warmup):
-        step(mode)
+        step()
     barrier()
     torch.cuda.synchronize()
     t_start = time.time()
-    ms = timed(lambda: step(mode), args.steps)
+    ms = _timed(step, args.steps)
     torch.cuda.synchronize()
     t_end = time.time()
     barrier()
@@ -244,60 +316,74 @@ def run_ours(args) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
-    # Per-shape times, plain FP32 vs the chosen mode, and cuSOLVER on the same GPU.
-    per_shape = {}
-    for (b, n), a, o in zip(SHAPES, data, outs):
-        per_shape[f"{b}x{n}"] = round(1000 * timed(lambda: cholesky(a, mode=mode, out=o), args.steps), 1)
-    plain = None
-    if mode not in (None, "fp32"):
-        plain = round(1000 * timed(lambda: step("fp32"), args.steps), 1)
-    cusolver = round(
-        1000 * timed(lambda: [torch.linalg.cholesky_ex(a, check_errors=False) for a in data], max(2, args.steps // 2)),
-        1,
-    )
+    extra = {}
+    if not args.quick:
+        # Per-shape times, the plain FP32 form, and cuSOLVER on the same GPU.
+        per_shape = {}
+        for j, ((b, n), m) in enumerate(zip(shapes, modes)):
+            a, o = sets[0][j], outs[0][j]
+            per_shape[f"{b}x{n}"] = round(1000 * _timed(lambda: cholesky(a, mode=m, out=o), args.steps), 1)
+        plain = None
+        if any(m != "fp32" for m in modes):
+            plain = round(1000 * _timed(lambda: eager_step(0, ["fp32"] * len(shapes)), args.steps), 1)
+        cus = round(
+            1000
+            * _timed(lambda: [torch.linalg.cholesky_ex(a, check_errors=False) for a in sets[0]], max(2, args.steps // 2)),
+            1,
+        )
+        # Accuracy at full size (FP64 on the device).
+        eager_step(0)
+        resid = {}
+        for (b, n), a, o in zip(shapes, sets[0], outs[0]):
+            ld, ad = o.double(), a.double()
+            r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - ad) / torch.linalg.matrix_norm(ad)
+            resid[f"{b}x{n}"] = float(r.max())
+        extra = {
+            "per_shape_us": per_shape,
+            "plain_fp32_us": plain,
+            "cusolver_same_gpu_us": cus,
+            "rel_residual_fro": resid,
+        }
 
-    # Accuracy at full size (FP64 on the device).
-    step(mode)
-    resid = {}
-    for (b, n), a, o in zip(SHAPES, data, outs):
-        ld = o.double()
-        ad = a.double()
-        r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - ad) / torch.linalg.matrix_norm(ad)
-        resid[f"{b}x{n}"] = float(r.max())
-
-    # Per-kernel device time of one step (CUDA events on the launch stream).
+    # Per-kernel device time of one eager step (CUDA events on the launch stream).
+    torch.cuda.synchronize()
     with _lib.LaunchTrace() as tr:
-        step(mode)
+        eager_step(0)
     totals = tr.totals()
     launches_per_step = sum(c for c, _ in totals.values())
-    dom = max(totals.items(), key=lambda kv: kv[1][1])
-    dom_name, (dom_count, dom_ms) = dom
-    peaks = _measured_peaks()
-    roof = _roofline(dom_name, dom_ms, dom_count, mode, peaks)
+    dom_name, (dom_count, dom_ms) = max(totals.items(), key=lambda kv: kv[1][1])
+    # The dominant kernel's share of one traced step, applied to the timed
+    # (graph-replayed) step time: its device time inside the timed region.
+    share = dom_ms / max(sum(t for _, t in totals.values()), 1e-12)
+    roof = _roofline(args.workload, shapes, dom_name, ms * share, dom_count, modes, _measured_peaks())
+    roof["share_of_step"] = round(share, 4)
 
     # End to end through the public API: pinned host in, host out, every step.
-    host_in = [a.cpu().pin_memory() for a in data]
-    host_out = [torch.empty_like(h).pin_memory() for h in host_in]
-    dev_in = [torch.empty_like(a) for a in data]
+    e2e = None
+    if not args.quick:
+        host_in = [a.cpu().pin_memory() for a in sets[0]]
+        host_out = [torch.empty_like(h).pin_memory() for h in host_in]
+        dev_in = [torch.empty_like(a) for a in sets[0]]
 
-    def e2e_step():
-        for hi, di, do, ho in zip(host_in, dev_in, outs, host_out):
-            di.copy_(hi, non_blocking=True)
-            cholesky(di, mode=mode, out=do)
-            ho.copy_(do, non_blocking=True)
+        def e2e_step():
+            for hi, di, do, ho, m in zip(host_in, dev_in, outs[0], host_out, modes):
+                di.copy_(hi, non_blocking=True)
+                cholesky(di, mode=m, out=do)
+                ho.copy_(do, non_blocking=True)
 
-    e2e_step()
-    torch.cuda.synchronize()
-    e2e_ms = timed(e2e_step, max(2, args.steps // 2))
-    h2d = sum(h.numel() * 4 for h in host_in)
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = _timed(e2e_step, max(2, args.steps // 2))
+        h2d = sum(h.numel() * 4 for h in host_in)
+        e2e = {"value": round(e2e_ms * 1000, 1), "unit": "us", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = _cpu_baseline(args)
+    if rank == 0 and ws == 1 and not args.no_cpu and not args.quick:
+        cpu = _cpu_baseline(args, wl)
 
     if rank == 0:
         line = {
-            "metric": METRIC,
+            "metric": wl["metric"],
             "value": round(ms * 1000, 1),
             "unit": "us",
             "n_gpus": ws,
@@ -307,34 +393,29 @@ def run_ours(args) -> int:
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32" if mode in (None, "fp32") else f"f32 ({mode} trailing updates)",
+            "dtype": "f32",
             "data": "synthetic",
             "config": {
-                "workload": WORKLOAD,
-                "shapes": [f"{b}x{n}" for b, n in SHAPES],
-                "mode": mode or "fp32",
-                "l2": "inputs (0.92 GB) larger than L2; no flush",
+                "workload": wl["desc"] + ("" if args.scale == 1.0 else f" (batch scaled x{args.scale})"),
+                "shapes": [f"{b}x{n}" for b, n in shapes],
+                "mode": args.mode,
+                "modes": dict(zip([f"{b}x{n}" for b, n in shapes], modes)),
+                "l2": "inputs larger than L2 (rotating sets where one set is smaller); no flush",
+                "timing": "CUDA-graph replay of one step, CUDA events, max over ranks",
                 "parallelism": f"weak scaling, {ws} rank(s) each a full step",
             },
-            "per_shape_us": per_shape,
-            "plain_fp32_us": plain,
-            "cusolver_same_gpu_us": cusolver,
-            "rel_residual_fro": resid,
-            "matrices_per_s": round(ws * sum(b for b, _ in SHAPES) / (ms / 1000.0), 1),
-            "gflops_per_s": round(ws * sum(_flops(b, n) for b, n in SHAPES) / (ms / 1000.0) / 1e9, 1),
+            **extra,
+            "matrices_per_s": round(ws * sum(b for b, _ in shapes) / (ms / 1000.0), 1),
+            "gflops_per_s": round(ws * sum(_flops(b, n) for b, n in shapes) / (ms / 1000.0) / 1e9, 1),
             "roofline": roof,
             "kernels_one_step": {k: {"launches": c, "ms": round(t, 4)} for k, (c, t) in sorted(totals.items())},
             "cpu_baseline": cpu,
-            "e2e": {
-                "value": round(e2e_ms * 1000, 1),
-                "unit": "us",
-                "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": h2d,
-            },
+            "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
         }
         print(json.dumps(line))
+    del graphs
     if ws > 1:
         import torch.distributed as dist
 
@@ -343,61 +424,69 @@ def run_ours(args) -> int:
     return 0
 
 
-def _roofline(name: str, ms: float, count: int, mode, peaks: dict) -> dict:
+def _roofline(workload: str, shapes, name: str, ms: float, count: int, modes, peaks: dict) -> dict:
     """Roofline of the dominant kernel over one step.
 
-    Algorithmic units: the trailing SYRK kernels count the flops of the lower
-    triangle they update, R(R+1)*nb per matrix and step (R = rows below the
-    block column, nb = 64); other kernels count FP32 bytes read + written.
+    Algorithmic units: HBM-bound kernels (the n <= 32 warp kernel) count 8*n^2
+    bytes per matrix (read A, write L once); factorization kernels count the
+    flops B*n^3/3 of the matrices they factor (the fused and CTA kernels) or,
+    for the trailing-update kernels of the blocked path, the flops of the
+    lower triangle they update, R(R+1)*64 per matrix and step.
     """
-    nb = 64
-    flops = 0.0
-    if name.startswith("trail"):
-        for b, n in SHAPES:
-            for k0 in range(0, n, nb):
-                r = n - k0 - nb
-                if r > 0:
-                    flops += b * r * (r + 1) * nb
-        achieved = flops / (ms / 1000.0) / 1e12
-        peak = peaks["bf16_tflops"]
-        tr = _profiled_traffic().get((name, str(mode or "fp32")))
+    traffic_tab = _profiled_traffic()
+    if name == "potrf_warp32_kernel":
+        byts = sum(8.0 * b * n * n for b, n in shapes)
+        achieved = byts / (ms / count / 1000.0) / 1e9
+        tpu = traffic_tab.get((name, workload, "fp32"))
         return {
             "kernel": name,
-            "bound": "tensor",
-            "achieved": round(achieved, 2),
-            "peak": peak,
-            "unit": "TFLOP/s",
-            "frac": round(achieved / peak, 4),
-            "peak_src": f"bf16 dense, {peaks['src']}",
-            "traffic": None if tr is None else round(tr * flops / max(count, 1)),
+            "bound": "hbm",
+            "achieved": round(achieved, 1),
+            "peak": peaks["hbm_gbs"],
+            "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "peak_src": "HBM copy " + peaks["src"],
+            "algorithmic_bytes_per_launch": byts,
+            "traffic": None if tpu is None else round(tpu * byts),
             "launches": count,
             "ms": round(ms, 4),
         }
-    byts = sum(8.0 * b * n * n for b, n in SHAPES)
-    achieved = byts / (ms / 1000.0) / 1e9
+    if name.startswith("trail"):
+        flops = 0.0
+        for b, n in shapes:
+            for k0 in range(0, n, 64):
+                r = n - k0 - 64
+                if r > 0:
+                    flops += b * r * (r + 1) * 64
+    else:
+        flops = sum(_flops(b, n) for b, n in shapes)
+    per_launch = flops / max(count, 1)
+    achieved = flops / (ms / 1000.0) / 1e12
+    mode = modes[-1]
+    tpu = traffic_tab.get((name, workload, mode))
     return {
         "kernel": name,
-        "bound": "hbm",
-        "achieved": round(achieved, 1),
-        "peak": peaks["hbm_gbs"],
-        "unit": "GB/s",
-        "frac": round(achieved / peaks["hbm_gbs"], 4),
-        "peak_src": peaks["src"],
-        "traffic": None,
+        "bound": "tensor",
+        "achieved": round(achieved, 3),
+        "peak": peaks["bf16_tflops"],
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peaks["bf16_tflops"], 5),
+        "peak_src": "dense BF16 cuBLAS " + peaks["src"] + " (algorithmic n^3/3 flops; BF16x3 issues 3 MMAs each)",
+        "algorithmic_flops_per_launch": per_launch,
+        "traffic": None if tpu is None else round(tpu * per_launch),
         "launches": count,
         "ms": round(ms, 4),
     }
 
 
-def _cpu_baseline(args) -> dict:
+def _cpu_baseline(args, wl) -> dict:
     """The reference's CPU route on a bounded sample, on all host cores."""
     import oracle
-    from gpumode_cholesky_b200 import inputs
 
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in SHAPES]
-    data = [inputs.mixed_batch(b, n, SEEDS[n], device="cpu") for b, n in sample]
+    sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+    data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for a in data:
         oracle.ref_kernel_cpu(a)
     reps = 2
@@ -406,7 +495,7 @@ def _cpu_baseline(args) -> dict:
         for a in data:
             oracle.ref_kernel_cpu(a)
     dt = (time.perf_counter() - t0) / reps
-    scale = sum(_flops(b, n) for b, n in SHAPES) / sum(_flops(b, n) for b, n in sample)
+    scale = sum(_flops(b, n) for b, n in wl["shapes"]) / sum(_flops(b, n) for b, n in sample)
     return {
         "value": round(dt * 1e6 * scale, 1),
         "unit": "us",
@@ -421,12 +510,15 @@ def _cpu_baseline(args) -> dict:
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", default="fp32")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mid")
+    ap.add_argument("--mode", default="auto")
     ap.add_argument("--ref-sample", type=float, default=0.05, help="fraction of the step the CPU legs factor")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true", help="timed region and roofline only (for profiling)")
+    ap.add_argument("--scale", type=float, default=1.0, help="batch scale (small profiling cases); 1 = the workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
