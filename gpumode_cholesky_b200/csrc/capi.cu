@@ -119,7 +119,14 @@ int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mo
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
-  if (fused_supported(n, mode)) return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+  if (fused_supported(n, mode)) {
+    // More matrices than SMs: two independent CTAs per SM hide each other's
+    // latency best; otherwise one warp-specialized CTA per matrix overlaps
+    // the next block column's update with the current panel.
+    if (batch > device_sms())
+      return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+    return potrf_fused_ws(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+  }
   return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
 }
 

@@ -24,6 +24,19 @@ namespace b2p {
 constexpr int kD64Ld = 68;   // row stride of S and T (floats)
 constexpr int kD64Threads = 128;
 
+// Barrier used between the engine's phases: the whole CTA, or a named
+// barrier over the first N threads (when other warps of the CTA run a
+// different role and must not be waited for).
+struct CtaBarrier {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+template <int NTHREADS>
+struct NamedBarrier1 {
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync 1, %0;" ::"n"(NTHREADS) : "memory");
+  }
+};
+
 struct Diag64Smem {
   float S[64 * kD64Ld];   // block: A in, L out (lower; upper zero)
   float T[64 * kD64Ld];   // inverse of L (lower; upper zero)
@@ -108,7 +121,8 @@ __device__ __forceinline__ int diag64_factor_block(Diag64Smem& sm, int r0, float
 // Returns the first bad pivot (0..63) or -1, uniform across the CTA.  Every
 // thread of the CTA must call it; threads beyond the first kD64Threads only
 // take part in the barriers.
-__device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
+template <class Bar = CtaBarrier>
+__device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm, Bar bar = Bar()) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -120,7 +134,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
     const int b = diag64_factor_block(sm, 0, sm.lt0, sm.invd, lane);
     if (lane == 0) sm.bad[0] = b;
   }
-  __syncthreads();
+  bar();
   if (warp == 1) {
     float x[32];
     const float* row = sm.S + (32 + lane) * kD64Ld;
@@ -145,7 +159,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) sm.T[j * kD64Ld + lane] = y[j];
   }
-  __syncthreads();
+  bar();
   if (active) {
     // A22 -= L21 L21^T (lower part): thread -> row i, 8 columns.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
@@ -171,12 +185,12 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
     for (int q = 0; q < 8; ++q)
       if (c0 + q <= i) row[q] -= s[q];
   }
-  __syncthreads();
+  bar();
   if (warp == 0) {
     const int b = diag64_factor_block(sm, 32, sm.lt1, sm.invd + 32, lane);
     if (lane == 0) sm.bad[1] = b;
   }
-  __syncthreads();
+  bar();
   if (warp == 1) {
     float y[32];
     col_inverse32(y, lane, sm.lt1, sm.invd + 32);
@@ -205,7 +219,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
 #pragma unroll
     for (int q = 0; q < 16; ++q) sm.w21[i * kLtLd + c0 + q] = s[q];
   }
-  __syncthreads();
+  bar();
   if (active) {
     // T21 = -T22 W: thread -> row i, 8 columns.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
@@ -230,7 +244,7 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) out[q] = -s[q];
   }
-  __syncthreads();
+  bar();
   const int b0 = sm.bad[0], b1 = sm.bad[1];
   return b0 >= 0 ? b0 : (b1 >= 0 ? 32 + b1 : -1);
 }
@@ -238,7 +252,8 @@ __device__ __forceinline__ int diag64_factor_invert(Diag64Smem& sm) {
 // Inverse only: T = L^{-1} of the lower-triangular 64x64 block already in
 // sm.S (diagonal and lower part valid; identity padding beyond the true
 // width).  Uses lt0/lt1/p21t/w21 as scratch.  All threads call it.
-__device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
+template <class Bar = CtaBarrier>
+__device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm, Bar bar = Bar()) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -254,7 +269,7 @@ __device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
     }
     if (tid < 64) sm.invd[tid] = 1.0f / sm.S[tid * kD64Ld + tid];
   }
-  __syncthreads();
+  bar();
   if (warp == 0) {
     float y[32];
     col_inverse32(y, lane, sm.lt0, sm.invd);
@@ -266,7 +281,7 @@ __device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
 #pragma unroll
     for (int j = 0; j < 32; ++j) sm.T[(32 + j) * kD64Ld + 32 + lane] = y[j];
   }
-  __syncthreads();
+  bar();
   if (active) {
     // W = L21 T11: thread -> row i, 8 columns.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
@@ -282,7 +297,7 @@ __device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) sm.w21[i * kLtLd + c0 + q] = sacc[q];
   }
-  __syncthreads();
+  bar();
   if (active) {
     // T21 = -T22 W.
     const int i = tid >> 2, c0 = (tid & 3) * 8;
@@ -299,7 +314,7 @@ __device__ __forceinline__ void diag64_invert_only(Diag64Smem& sm) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) out[q] = -sacc[q];
   }
-  __syncthreads();
+  bar();
 }
 
 }  // namespace b2p

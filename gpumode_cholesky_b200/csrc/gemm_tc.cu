@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(GemmArgs g, int t
     const float* X = g.x + b * g.sx;
     const float* Y = g.y + b * g.sy;
     float* C = g.c + b * g.sc;
+    const float* Cin = (g.c_in ? g.c_in : g.c) + b * g.sc;
     bool any = false;
     for (int k0 = klo; k0 < khi; k0 += kGK) {
       // A operand: rows m (op1(X)[m][k]); B operand: rows n (op2(Y)[k][n]).
@@ -207,13 +208,14 @@ __global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(GemmArgs g, int t
       }
       if (i < g.m) {
         float* crow = C + (size_t)i * g.ldc;
+        const float* cin = Cin + (size_t)i * g.ldc;
 #pragma unroll
         for (int e = 0; e < 32; ++e) {
           const int j = n0 + 32 * ch + e;
           if (j < g.n && (!g.lower_out || j <= i)) {
             float r = g.alpha * v[e];
             if (g.phi) r = (j > i) ? 0.0f : (j == i ? 0.5f * r : r);
-            if (g.beta != 0.0f) r += g.beta * crow[j];
+            if (g.beta != 0.0f) r += g.beta * cin[j];
             crow[j] = r;
           }
         }

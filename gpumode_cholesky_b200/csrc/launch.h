@@ -33,7 +33,7 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
 // lower 128x128 tiles per matrix; ragged: one CTA per item of `sch`.
 int T_tc(int n, int k0);
 int launch_syrk_tc(const float* csrc, float* l, const Sched& sch, bool ragged, int tiles, int k0, int mode,
-                   int32_t* info, cudaStream_t s);
+                   int32_t* info, cudaStream_t s, int jmax = 0);
 int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const RaggedStep& st, int k0, int mode,
                         float* tws, int32_t* info, cudaStream_t s);
 
@@ -42,6 +42,9 @@ bool fused_supported(int64_t n, int mode);
 size_t fused_workspace_bytes(int64_t batch, int64_t n);
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s);
+// Warp-specialized variant (potrf_fused_ws.cu): same workspace and contract.
+int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
+                   int32_t* info, cudaStream_t s);
 
 // Batched tensor-core GEMM with structure hints (gemm_tc.cu):
 // C = alpha * op1(X) op2(Y) + beta * C per batch item.
@@ -58,6 +61,7 @@ struct GemmArgs {
   int phi;               // epilogue: zero above the diagonal, halve the diagonal
   float alpha, beta;
   int64_t batch;
+  const float* c_in;     // C read from here (null: from c); same layout as c
 };
 int launch_gemm_tc(const GemmArgs& g, int mode, int32_t* err, cudaStream_t s);
 
@@ -82,6 +86,7 @@ enum KernelId {
   kKBwdTrsm,
   kKBwdSym,
   kKFused,
+  kKFusedWs,
   kKCount
 };
 
@@ -116,6 +121,8 @@ enum SmemSlot {
   kSlotTrailR,
   kSlotTcR0,
   kSlotTcR1,
+  kSlotFusedWs0,
+  kSlotFusedWs1,
   kSlotCount
 };
 

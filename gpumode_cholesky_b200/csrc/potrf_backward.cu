@@ -67,6 +67,7 @@ static GemmArgs gemm_args(int64_t batch, int n) {
   g.alpha = 1.0f;
   g.beta = 0.0f;
   g.batch = batch;
+  g.c_in = nullptr;
   return g;
 }
 

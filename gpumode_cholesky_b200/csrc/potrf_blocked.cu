@@ -5,10 +5,11 @@
 //
 //   diag   one CTA per matrix: factor the 64x64 diagonal block and invert it
 //          in shared memory (diag64.cuh); write L_kk (zeros above its
-//          diagonal), zero the strictly-upper strip to the right of the
-//          block, and store T^T = inv(L_kk)^T in the workspace;
+//          diagonal) and store T = inv(L_kk) (row-major) in the workspace;
 //   panel  L[i, k0:k0+64] <- A[i, k0:k0+64] * T^T for the rows below
-//          (the TRSM as a GEMM against the explicit inverse);
+//          (the TRSM as a GEMM against the explicit inverse); CTA t also
+//          zeroes the 64x64 block t of the strictly-upper strip to the right
+//          of the diagonal block, so the strip is cleared by the whole grid;
 //   trail  C[i, j] -= sum_m L[i, k0+m] L[j, k0+m] over the lower 64x64 tiles
 //          of the trailing matrix (the SYRK).
 //
@@ -34,6 +35,13 @@ constexpr int kNB = 64;             // block column width
 constexpr int kTile = 64;           // panel rows / trailing tile edge per CTA
 constexpr int kGemmLd = kTile + 4;  // 68
 constexpr int kMaxGridY = 65535;
+constexpr int kOuterNB = 256;  // outer block column of the two-level schedule
+// Orders that use the two-level schedule (tensor modes).  Its K = 256 update
+// runs through gemm_tc_kernel, whose per-chunk staging is not yet faster
+// than the single-level tcgen05 SYRK on any measured order (1x8192: 10.9 vs
+// 10.3 ms), so the threshold is above every order the library accepts until
+// that kernel streams its operands.
+constexpr int kTwoLevelMin = 1 << 21;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -99,31 +107,39 @@ __global__ void __launch_bounds__(kD64Threads, 4)
     }
     __syncthreads();
     const int bad = diag64_factor_invert(sm);
-    // L_kk with zeros above its diagonal.
-    for (int e = tid; e < 64 * 64; e += kD64Threads) {
-      const int r = e >> 6, c = e & 63;
-      if (r < w && c < w) base[(size_t)r * n + c] = sm.S[r * kD64Ld + c];
-    }
-    // Strictly-upper strip right of the block: rows k0..k0+w, cols k0+64..n.
-    const int strip = n - k0 - kNB;
-    if (strip > 0) {
-      if (vec) {
-        const int s4 = strip >> 2;
-        for (int e = tid; e < w * s4; e += kD64Threads) {
-          const int r = e / s4, q = e - (e / s4) * s4;
-          reinterpret_cast<float4*>(base + (size_t)r * n + kNB)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      } else {
-        for (int e = tid; e < w * strip; e += kD64Threads) {
-          const int r = e / strip, c = e - (e / strip) * strip;
-          base[(size_t)r * n + kNB + c] = 0.0f;
+    // L_kk (zeros above its diagonal; the engine leaves them in S).
+    if (vec) {
+#pragma unroll
+      for (int it = 0; it < 8; ++it) {
+        const int e4 = tid + kD64Threads * it;
+        const int r = e4 >> 4, c = (e4 & 15) * 4;
+        if (r < w && c < w) {
+          const float* sr = sm.S + r * kD64Ld + c;
+          *reinterpret_cast<float4*>(base + (size_t)r * n + c) =
+              make_float4(c <= r ? sr[0] : 0.f, c + 1 <= r ? sr[1] : 0.f, c + 2 <= r ? sr[2] : 0.f,
+                          c + 3 <= r ? sr[3] : 0.f);
         }
       }
+    } else {
+      for (int e = tid; e < 64 * 64; e += kD64Threads) {
+        const int r = e >> 6, c = e & 63;
+        if (r < w && c < w) base[(size_t)r * n + c] = (c <= r) ? sm.S[r * kD64Ld + c] : 0.0f;
+      }
     }
+    // T = inv(L_kk), row-major (the panel kernel transposes it on load).
     float* tb = tws + b * kNB * kNB;
-    for (int e = tid; e < kNB * kNB; e += kD64Threads) {
-      const int m = e >> 6, c = e & 63;
-      tb[e] = (m < w && c < w) ? sm.T[c * kD64Ld + m] : 0.0f;  // T^T[m][c] = T[c][m]
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      const int e4 = tid + kD64Threads * it;
+      const int r = e4 >> 4, c = (e4 & 15) * 4;
+      const float* tr = sm.T + r * kD64Ld + c;
+      float4 v = make_float4(tr[0], tr[1], tr[2], tr[3]);
+      if (r >= w) v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (c + 0 >= w) v.x = 0.f;
+      if (c + 1 >= w) v.y = 0.f;
+      if (c + 2 >= w) v.z = 0.f;
+      if (c + 3 >= w) v.w = 0.f;
+      reinterpret_cast<float4*>(tb)[e4] = v;
     }
     if (info != nullptr && tid == 0) {
       if (k0 == 0) info[tg.mat] = bad >= 0 ? bad + 1 : 0;
@@ -206,15 +222,26 @@ __global__ void __launch_bounds__(kGemmThreads)
     const int row0 = k0 + kNB + tg.ti * kTile;
     const size_t moff = tg.off;
     const float* tb = tws + tg.pos * kNB * kNB;
+    // Ts[m][c] = T[c][m]: consecutive threads take consecutive rows c of T,
+    // so the transposed stores are bank-conflict free.
+    {
+      float4 tv[16];
 #pragma unroll
-    for (int it = 0; it < 16; ++it) {
-      const int e = tid + kGemmThreads * it;
-      const int m = e >> 4, q = e & 15;
-      cp_async16(Ts + m * kGemmLd + 4 * q, tb + m * kNB + 4 * q);
+      for (int it = 0; it < 16; ++it) {
+        const int e = tid + kGemmThreads * it;
+        tv[it] = __ldg(reinterpret_cast<const float4*>(tb) + (e & 63) * 16 + (e >> 6));
+      }
+      load_rows_t(src + moff, n, row0, k0, Ps);
+#pragma unroll
+      for (int it = 0; it < 16; ++it) {
+        const int e = tid + kGemmThreads * it;
+        const int c = e & 63, q = e >> 6;
+        Ts[(4 * q + 0) * kGemmLd + c] = tv[it].x;
+        Ts[(4 * q + 1) * kGemmLd + c] = tv[it].y;
+        Ts[(4 * q + 2) * kGemmLd + c] = tv[it].z;
+        Ts[(4 * q + 3) * kGemmLd + c] = tv[it].w;
+      }
     }
-    cp_async_commit();
-    load_rows_t(src + moff, n, row0, k0, Ps);
-    cp_async_wait_all();
     __syncthreads();
     float acc[8][8];
     tile_mma_8x8(Ps, Ts, ty, tx, acc);
@@ -230,6 +257,24 @@ __global__ void __launch_bounds__(kGemmThreads)
         } else {
 #pragma unroll
           for (int c = 0; c < 8; ++c) dst[slot_index(tx, c)] = acc[r][c];
+        }
+      }
+    }
+    // Zero block ti of the strip: rows k0..k0+63, cols k0+64+64*ti .. +63.
+    {
+      const int c0 = k0 + kNB + tg.ti * kTile;
+      const int cw = min(kTile, n - c0);
+      float* zb = mat + (size_t)k0 * n + c0;
+      if ((n & 3) == 0) {
+        const int q4 = cw >> 2;
+        for (int e = tid; e < kNB * q4; e += kGemmThreads) {
+          const int r = e / q4, q = e - (e / q4) * q4;
+          reinterpret_cast<float4*>(zb + (size_t)r * n)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      } else {
+        for (int e = tid; e < kNB * cw; e += kGemmThreads) {
+          const int r = e / cw, c = e - (e / cw) * cw;
+          zb[(size_t)r * n + c] = 0.0f;
         }
       }
     }
@@ -337,31 +382,59 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
   if (int st = ensure_smem_attr((const void*)trail_kernel<false>, tsmem, kSlotTrail)) return st;
   const int gy = (int)std::min<int64_t>(batch, kMaxGridY);
   const Sched sch = dense_sched(batch, n);
-  for (int k0 = 0; k0 < n; k0 += kNB) {
-    const float* src = (k0 == 0) ? a : l;
-    const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
-    {
-      TraceScope ts(kKDiag, s);
-      diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
+  // Tensor modes on large orders: two-level blocking.  Inner 64-wide steps
+  // factor a 256-wide block column (their trailing updates limited to its
+  // columns); one tcgen05 SYRK with K = 256 then updates the rest.
+  const int outer = (tensor && n >= kTwoLevelMin) ? kOuterNB : n;
+  for (int K0 = 0; K0 < n; K0 += outer) {
+    const int jmax = std::min(n, K0 + outer);
+    for (int k0 = K0; k0 < jmax; k0 += kNB) {
+      const float* src = (k0 == 0) ? a : l;
+      const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
+      {
+        TraceScope ts(kKDiag, s);
+        diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
+      }
+      if (int st = check_launch("diag_kernel")) return st;
+      const int R = n - k0 - kNB;
+      if (R <= 0) return B2P_OK;
+      const int T = (R + kTile - 1) / kTile;
+      {
+        TraceScope ts(kKPanel, s);
+        panel_kernel<false><<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, sch, k0, tws);
+      }
+      if (int st = check_launch("panel_kernel")) return st;
+      if (k0 + kNB >= jmax) continue;
+      if (tensor) {
+        if (int st = launch_syrk_tc(src, l, sch, false, T_tc(n, k0), k0, mode, info, s, jmax < n ? jmax : 0))
+          return st;
+        continue;
+      }
+      {
+        TraceScope ts(kKTrail, s);
+        trail_kernel<false><<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0);
+      }
+      if (int st = check_launch("trail_kernel")) return st;
     }
-    if (int st = check_launch("diag_kernel")) return st;
-    const int R = n - k0 - kNB;
-    if (R <= 0) break;
-    const int T = (R + kTile - 1) / kTile;
-    {
-      TraceScope ts(kKPanel, s);
-      panel_kernel<false><<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, sch, k0, tws);
+    if (jmax < n) {
+      // C[jmax:, jmax:] -= X X^T, X = L[jmax:, K0:jmax] (lower triangle only).
+      const size_t nn = (size_t)n;
+      GemmArgs g{};
+      g.x = l + (size_t)jmax * nn + K0;
+      g.y = g.x;
+      g.c = l + (size_t)jmax * nn + jmax;
+      g.c_in = ((K0 == 0) ? a : l) + (size_t)jmax * nn + jmax;
+      g.sx = g.sy = g.sc = (int64_t)n * n;
+      g.ldx = g.ldy = g.ldc = n;
+      g.m = g.n = n - jmax;
+      g.k = jmax - K0;
+      g.trans_y = 1;
+      g.lower_out = 1;
+      g.alpha = -1.0f;
+      g.beta = 1.0f;
+      g.batch = batch;
+      if (int st = launch_gemm_tc(g, mode, nullptr, s)) return st;
     }
-    if (int st = check_launch("panel_kernel")) return st;
-    if (tensor) {
-      if (int st = launch_syrk_tc(src, l, sch, false, T_tc(n, k0), k0, mode, info, s)) return st;
-      continue;
-    }
-    {
-      TraceScope ts(kKTrail, s);
-      trail_kernel<false><<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0);
-    }
-    if (int st = check_launch("trail_kernel")) return st;
   }
   return B2P_OK;
 }

@@ -30,6 +30,7 @@
 #include "diag64.cuh"
 #include "launch.h"
 #include "umma.cuh"
+#include "xgemm.cuh"
 
 namespace b2p {
 
@@ -317,40 +318,20 @@ __global__ void __launch_bounds__(kFThreads, 2)
           }
           __syncthreads();
         }
-        // X = P T^T for the rows below the diagonal block.
-        {
-          const int ty = tid >> 3, tx = tid & 7;
-          const bool skip = (mt == 0 && ty < 16);  // rows 0..63 of tile 0 are the diagonal block
-          if (!skip) {
-            float acc[4][8];
+        // X = P T^T for the rows below the diagonal block (triangle skipped),
+        // then L and the tensor-core copy from X^T.
+        xgemm_tri_inplace(PtT, kFPtLd, TT, kFTtLd, CtaBarrier());
+        for (int item = tid; item < kFM * 8; item += kFThreads) {
+          const int rl = item & (kFM - 1), c = item >> 7;
+          if (rl >= vr || (mt == 0 && rl < 64)) continue;
+          float v[8];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-              for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
-#pragma unroll 4
-            for (int m = 0; m < kFB; ++m) {
-              const float4 av = *reinterpret_cast<const float4*>(PtT + m * kFPtLd + 4 * ty);
-              const float4 b0 = *reinterpret_cast<const float4*>(TT + m * kFTtLd + 8 * tx);
-              const float4 b1 = *reinterpret_cast<const float4*>(TT + m * kFTtLd + 8 * tx + 4);
-              const float a4[4] = {av.x, av.y, av.z, av.w};
-              const float b8[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-              for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a4[i], b8[j], acc[i][j]);
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int rl = 4 * ty + i;
-              if (rl < vr) {
-                const int rg = r0 + rl;
-                float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * tx);
-                dst[0] = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
-                dst[1] = make_float4(acc[i][4], acc[i][5], acc[i][6], acc[i][7]);
-                if (k + 1 < N) fused_store_ws<MODE>(W0, W1, N, k, rg, tx, acc[i]);
-              }
-            }
-          }
+          for (int j = 0; j < 8; ++j) v[j] = PtT[(8 * c + j) * kFPtLd + rl];
+          const int rg = r0 + rl;
+          float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * c);
+          dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+          dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+          if (k + 1 < N) fused_store_ws<MODE>(W0, W1, N, k, rg, c, v);
         }
         __syncthreads();
       }

@@ -1,0 +1,436 @@
+// Warp-specialized fused left-looking factorization on the tensor cores.
+//
+// Same dataflow as potrf_fused.cu (one CTA per matrix, A read once, L written
+// once, update accumulated in TMEM from pre-swizzled panel copies), but the
+// update of block column k+1 runs concurrently with the panel work of block
+// column k:
+//
+//   warp 8 (producer, one thread)  streams the panel copies with
+//        cp.async.bulk (two stages) and issues the tcgen05 MMAs of the next
+//        block column tile by tile; per tile it commits `acc_ready`;
+//   warps 0-7 (consumers)  per tile: wait `acc_ready`, read D from TMEM
+//        (then arrive `acc_free`), P = A - D, factor + invert the diagonal
+//        block (tile 0), X = P T^T in FP32, write L and the tensor-core copy
+//        of X, then arrive `tile_ready`.
+//
+// Ordering rules (every mbarrier is waited at most one phase behind):
+//   * MMA write #w into TMEM tile t waits for consumer read #(w-1) of t;
+//   * the update of block column k, tile t, over column k-1 needs the panel
+//     rows of column k-1 produced by consumer tiles {0, t, t+1} of step k-1;
+//     older columns are ready, so their MMAs are issued first.
+// All waits are bounded; a timeout sets a shared flag that both roles check,
+// marks the matrix with info = -1 and drains outstanding copies and MMAs
+// before TMEM is released.
+//
+// The reference's left-looking paths (submission.py:3319-3409, 3606-3676,
+// 5152-5196) issue the same three phases as separate cuSOLVER / cuBLAS /
+// CUDA calls with host round trips between them.
+#include <algorithm>
+
+#include "diag64.cuh"
+#include "launch.h"
+#include "umma.cuh"
+#include "xgemm.cuh"
+
+namespace b2p {
+
+constexpr int kWConsumers = 256;
+constexpr int kWThreads = kWConsumers + 32;
+constexpr int kWB = 64;
+constexpr int kWM = 128;
+constexpr int kWPtLd = 132;
+constexpr int kWTtLd = 68;
+constexpr uint32_t kWPolls = 1u << 24;
+constexpr uint32_t kWTmemCols = 512;
+
+constexpr uint32_t kWStageA = 32768;
+constexpr uint32_t kWStage = kWStageA + 16384;
+constexpr uint32_t kWDiagOff = 2 * kWStage;
+constexpr uint32_t kWPtOff = kWDiagOff + (((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u);
+constexpr uint32_t kWTtOff = kWPtOff + 64 * kWPtLd * 4;
+constexpr uint32_t kWBarOff = kWTtOff + 64 * kWTtLd * 4;
+constexpr uint32_t kWSmemBytes = kWBarOff + 256 + 1024;
+
+using ConsumerBar = NamedBarrier1<kWConsumers>;
+
+__device__ __forceinline__ size_t ws_row_byte(int N, int c, int r) {
+  return (size_t)(64 * (c * (N - 1) - c * (c - 1) / 2) + r - 64 * (c + 1)) * 128;
+}
+
+__device__ __forceinline__ float ws_round_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(mbar)) : "memory");
+}
+
+// Bounded wait that also gives up when the other role has flagged a failure.
+__device__ __forceinline__ bool ws_wait(uint64_t* mbar, uint32_t parity, volatile int* flag) {
+  for (uint32_t i = 0; i < kWPolls; ++i) {
+    if (umma::mbar_try_wait(mbar, parity)) return true;
+    if ((i & 255u) == 255u && *flag) return false;
+  }
+  return false;
+}
+
+template <int MODE>
+__device__ __forceinline__ void ws_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
+  if (MODE == B2P_MODE_TF32) {
+    constexpr uint32_t idesc = umma::idesc_f32acc(2, kWM, kWB);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
+      const uint32_t kb = (uint32_t)((s >> 2) * 8192 + (s & 3) * 32);
+      umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
+    }
+  } else {
+    constexpr uint32_t idesc = umma::idesc_f32acc(1, kWM, kWB);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const uint32_t o = (uint32_t)(s * 32);
+      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
+      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + 8192 + o);
+      umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
+      umma::mma_bf16(d, ah, bl, idesc, 1u);
+      umma::mma_bf16(d, ah, bh, idesc, 1u);
+    }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void ws_store_copy(uint8_t* w0, uint8_t* w1, int N, int c, int r, int tx,
+                                              const float (&v)[8]) {
+  const size_t row = ws_row_byte(N, c, r);
+  const int r8 = r & 7;
+  if (MODE == B2P_MODE_TF32) {
+    uint8_t* reg = (tx < 4) ? w0 : w1;
+    const int c0 = 2 * (tx & 3);
+    *reinterpret_cast<float4*>(reg + row + ((c0 ^ r8) << 4)) =
+        make_float4(ws_round_tf32(v[0]), ws_round_tf32(v[1]), ws_round_tf32(v[2]), ws_round_tf32(v[3]));
+    *reinterpret_cast<float4*>(reg + row + (((c0 + 1) ^ r8) << 4)) =
+        make_float4(ws_round_tf32(v[4]), ws_round_tf32(v[5]), ws_round_tf32(v[6]), ws_round_tf32(v[7]));
+  } else {
+    uint32_t h[4], lo[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      umma::split_bf16(v[2 * p], h0, l0);
+      umma::split_bf16(v[2 * p + 1], h1, l1);
+      h[p] = umma::pack_bf16(h0, h1);
+      lo[p] = umma::pack_bf16(l0, l1);
+    }
+    const size_t off = row + ((tx ^ r8) << 4);
+    *reinterpret_cast<uint4*>(w0 + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(w1 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
+struct WsBars {
+  uint64_t* full;        // [2]
+  uint64_t* empty;       // [2]
+  uint64_t* acc_ready;   // [8]
+  uint64_t* acc_free;    // [8]
+  uint64_t* tile_ready;  // [8]
+  uint64_t* drain;       // [1]
+  uint32_t* tslot;
+  volatile int* flag;
+  int* badp;
+};
+
+// ---------------------------------------------------------------------------
+// Producer: one thread.
+template <int MODE>
+__device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t batch, int n, uint32_t tmem) {
+  const int N = n / kWB;
+  const size_t rbytes = (size_t)4096 * N * (N - 1);
+  uint32_t n_load[2] = {0u, 0u}, n_empty[2] = {0u, 0u};
+  int writes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t biter = 0;
+  bool ok = true;
+  for (int64_t b = blockIdx.x; b < batch && ok; b += gridDim.x, ++biter) {
+    const uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
+    const uint8_t* W1 = W0 + rbytes;
+    for (int k = 1; k < N && ok; ++k) {
+      const int k0 = k * kWB;
+      const int mt_n = (n - k0 + kWM - 1) / kWM;
+      const int prev_n = (n - k0 + kWB + kWM - 1) / kWM;
+      const int iters = mt_n * k;
+      // Dependencies of the chunk over column k-1 for tile mt.
+      auto deps_ready = [&](int mt, bool block) -> bool {
+        int ts[3];
+        int nt = 0;
+        if (mt == 0) ts[nt++] = 0;
+        if (mt != 0) ts[nt++] = mt;
+        if (mt + 1 < prev_n) ts[nt++] = mt + 1;
+        for (int q = 0; q < nt; ++q) {
+          const int t = ts[q];
+          const int64_t idx = biter * (int64_t)(N - 2 * t) + (k - 1);
+          const uint32_t par = (uint32_t)(idx & 1);
+          if (block) {
+            if (!ws_wait(br.tile_ready + t, par, br.flag)) return false;
+          } else if (!umma::mbar_try_wait(br.tile_ready + t, par)) {
+            return false;
+          }
+        }
+        return true;
+      };
+      auto issue_load = [&](int i) -> bool {
+        const int mt = i / k, kc = i - (i / k) * k;
+        const int s = i & 1;
+        if (n_load[s] > 0) {
+          // The stage held the previous chunk: wait until the MMAs that read it completed.
+          if (!ws_wait(br.empty + s, (n_load[s] - 1u) & 1u, br.flag)) return false;
+        }
+        if (kc == k - 1 && !deps_ready(mt, true)) return false;
+        const int r0 = k0 + mt * kWM;
+        const uint32_t abytes = (uint32_t)min(kWM, n - r0) * 128u;
+        const size_t aoff = ws_row_byte(N, kc, r0);
+        const size_t boff = ws_row_byte(N, kc, k0);
+        uint8_t* st = sm + s * kWStage;
+        umma::mbar_arrive_expect_tx(br.full + s, 2 * abytes + 2 * 8192u);
+        umma::bulk_g2s(st, W0 + aoff, abytes, br.full + s);
+        umma::bulk_g2s(st + 16384, W1 + aoff, abytes, br.full + s);
+        umma::bulk_g2s(st + kWStageA, W0 + boff, 8192u, br.full + s);
+        umma::bulk_g2s(st + kWStageA + 8192, W1 + boff, 8192u, br.full + s);
+        ++n_load[s];
+        return true;
+      };
+      int next = 0;
+      if (iters > 0) {
+        if (!issue_load(0)) { ok = false; break; }
+        next = 1;
+      }
+      for (int i = 0; i < iters && ok; ++i) {
+        const int s = i & 1;
+        const int mt = i / k, kc = i - (i / k) * k;
+        // Prefetch the next chunk unless it would wait on consumers.
+        bool prefetched = false;
+        if (next == i + 1 && next < iters) {
+          const int nmt = next / k, nkc = next - (next / k) * k;
+          if (nkc != k - 1 || deps_ready(nmt, false)) {
+            if (!issue_load(next)) { ok = false; break; }
+            ++next;
+            prefetched = true;
+          }
+        }
+        if (!ws_wait(br.full + s, (n_load[s] - 1u) & 1u, br.flag)) { ok = false; break; }
+        if (kc == 0 && writes[mt] > 0) {
+          // TMEM tile mt must have been read by the consumers.
+          if (!ws_wait(br.acc_free + mt, (uint32_t)((writes[mt] - 1) & 1), br.flag)) { ok = false; break; }
+        }
+        umma::fence_after_sync();
+        const uint32_t st = umma::smem_u32(sm + s * kWStage);
+        ws_mmas<MODE>(tmem + (uint32_t)(kWB * mt), st, st + kWStageA, kc > 0);
+        umma::mma_commit(br.empty + s);
+        ++n_empty[s];
+        if (kc == k - 1) {
+          umma::mma_commit(br.acc_ready + mt);
+          ++writes[mt];
+        }
+        if (!prefetched && next == i + 1 && next < iters) {
+          if (!issue_load(next)) { ok = false; break; }
+          ++next;
+        }
+      }
+    }
+  }
+  if (!ok) *br.flag = 1;
+  // Drain: every copy lands and every MMA completes before TMEM is released.
+  for (int s = 0; s < 2; ++s) {
+    if (n_load[s] > 0) umma::mbar_wait_bounded(br.full + s, (n_load[s] - 1u) & 1u, kWPolls);
+  }
+  umma::mma_commit(br.drain);
+  umma::mbar_wait_bounded(br.drain, 0u, kWPolls);
+}
+
+// ---------------------------------------------------------------------------
+// Consumers: warps 0-7.
+template <int MODE>
+__device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
+                             int n, uint32_t tmem, int32_t* info) {
+  const ConsumerBar cbar;
+  Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
+  float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
+  float* TT = reinterpret_cast<float*>(sm + kWTtOff);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = n / kWB;
+  const size_t rbytes = (size_t)4096 * N * (N - 1);
+  uint32_t ready_par = 0u;  // bit t: parity of the next acc_ready phase of tile t
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const float* A = a + (size_t)b * n * n;
+    float* L = l + (size_t)b * n * n;
+    uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
+    uint8_t* W1 = W0 + rbytes;
+    if (tid == 0) *br.badp = -1;
+    bool failed = false;
+    for (int k = 0; k < N && !failed; ++k) {
+      const int k0 = k * kWB;
+      const int mt_n = (n - k0 + kWM - 1) / kWM;
+      for (int mt = 0; mt < mt_n; ++mt) {
+        const int r0 = k0 + mt * kWM;
+        const int vr = min(kWM, n - r0);
+        // (a) D from TMEM, P = A - D.
+        {
+          const int w4 = warp & 3, h = warp >> 2;
+          const int rl = 32 * w4 + lane;
+          float d[32];
+          if (k > 0) {
+            const bool got = ws_wait(br.acc_ready + mt, (ready_par >> mt) & 1u, br.flag);
+            ready_par ^= 1u << mt;
+            if (!got) *br.flag = 1;
+          }
+          cbar();
+          if (*br.flag) {
+            failed = true;
+            break;
+          }
+          if (k > 0) {
+            umma::fence_after_sync();
+            umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kWB * mt + 32 * h), d);
+            umma::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(br.acc_free + mt);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) d[q] = 0.0f;
+          }
+          float p[32];
+          if (rl < vr) {
+            const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + 32 * h);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float4 v = src[q];
+              p[4 * q + 0] = v.x - d[4 * q + 0];
+              p[4 * q + 1] = v.y - d[4 * q + 1];
+              p[4 * q + 2] = v.z - d[4 * q + 2];
+              p[4 * q + 3] = v.w - d[4 * q + 3];
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) p[q] = 0.0f;
+          }
+#pragma unroll
+          for (int q = 0; q < 32; ++q) PtT[(32 * h + q) * kWPtLd + rl] = p[q];
+          if (mt == 0 && rl < 64) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
+          }
+        }
+        cbar();
+        // (b) diagonal block: factor, invert, T^T, L_kk, zero strip.
+        if (mt == 0) {
+          const int bad = diag64_factor_invert(dg, cbar);
+          if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
+          for (int e = tid; e < 64 * 64; e += kWConsumers) {
+            const int m = e >> 6, c = e & 63;
+            TT[m * kWTtLd + c] = dg.T[c * kD64Ld + m];
+          }
+          for (int e = tid; e < 64 * 16; e += kWConsumers) {
+            const int r = e >> 4, c = (e & 15) * 4;
+            const float* srow = dg.S + r * kD64Ld + c;
+            const float4 v = make_float4(c <= r ? srow[0] : 0.f, c + 1 <= r ? srow[1] : 0.f,
+                                         c + 2 <= r ? srow[2] : 0.f, c + 3 <= r ? srow[3] : 0.f);
+            *reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + c) = v;
+          }
+          const int s4 = (n - k0 - kWB) >> 2;
+          for (int e = tid; e < 64 * s4; e += kWConsumers) {
+            const int r = e / s4, q = e - (e / s4) * s4;
+            reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + kWB)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+          cbar();
+        }
+        // (c) X = P T^T (triangle skipped), then L and the tensor-core copy from X^T.
+        xgemm_tri_inplace(PtT, kWPtLd, TT, kWTtLd, cbar);
+        for (int item = tid; item < kWM * 8; item += kWConsumers) {
+          const int rl = item & (kWM - 1), c = item >> 7;
+          if (rl >= vr || (mt == 0 && rl < 64)) continue;
+          float v[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[j] = PtT[(8 * c + j) * kWPtLd + rl];
+          const int rg = r0 + rl;
+          float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * c);
+          dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+          dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+          if (k + 1 < N) ws_store_copy<MODE>(W0, W1, N, k, rg, c, v);
+        }
+        // Publish this tile's panel rows to the producer's bulk copies.
+        umma::fence_proxy_async_all();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(br.tile_ready + mt);
+        cbar();
+      }
+    }
+    if (tid == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
+    if (failed) break;
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kWThreads, 1)
+    potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
+                          uint8_t* __restrict__ ws, int32_t* __restrict__ info) {
+  extern __shared__ unsigned char wraw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wraw) + 1023) & ~(uintptr_t)1023);
+  WsBars br;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kWBarOff);
+  br.full = bars;
+  br.empty = bars + 2;
+  br.acc_ready = bars + 4;
+  br.acc_free = bars + 12;
+  br.tile_ready = bars + 20;
+  br.drain = bars + 28;
+  br.tslot = reinterpret_cast<uint32_t*>(bars + 29);
+  br.flag = reinterpret_cast<volatile int*>(bars + 30);
+  br.badp = reinterpret_cast<int*>(bars + 30) + 1;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) *br.flag = 0;
+  if (warp == 0) {
+    umma::tmem_alloc(br.tslot, kWTmemCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 32) {
+    for (int i = 0; i < 4; ++i) umma::mbar_init(bars + i, 1);             // full, empty
+    for (int i = 0; i < 8; ++i) umma::mbar_init(br.acc_ready + i, 1);     // tcgen05.commit
+    for (int i = 0; i < 8; ++i) umma::mbar_init(br.acc_free + i, 8);      // one arrive per consumer warp
+    for (int i = 0; i < 8; ++i) umma::mbar_init(br.tile_ready + i, 8);
+    umma::mbar_init(br.drain, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *br.tslot;
+  if (warp == kWConsumers / 32) {
+    if ((tid & 31) == 0) ws_producer<MODE>(br, sm, ws, batch, n, tmem);
+  } else {
+    ws_consumers<MODE>(br, sm, a, l, ws, batch, n, tmem, info);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kWTmemCols);
+}
+
+int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
+                   int32_t* info, cudaStream_t s) {
+  const size_t need = fused_workspace_bytes(batch, n);
+  if (ws == nullptr || ws_bytes < need)
+    return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
+  uint8_t* wsa = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ws) + 1023) & ~(uintptr_t)1023);
+  const int grid = (int)std::min<int64_t>(batch, (int64_t)device_sms());
+  TraceScope ts(kKFusedWs, s);
+  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
+    if (int st = ensure_smem_attr((const void*)potrf_fused_ws_kernel<B2P_MODE_TF32>, kWSmemBytes, kSlotFusedWs0))
+      return st;
+    potrf_fused_ws_kernel<B2P_MODE_TF32><<<grid, kWThreads, kWSmemBytes, s>>>(a, l, batch, n, wsa, info);
+  } else {
+    if (int st = ensure_smem_attr((const void*)potrf_fused_ws_kernel<B2P_MODE_BF16X3>, kWSmemBytes, kSlotFusedWs1))
+      return st;
+    potrf_fused_ws_kernel<B2P_MODE_BF16X3><<<grid, kWThreads, kWSmemBytes, s>>>(a, l, batch, n, wsa, info);
+  }
+  return check_launch("potrf_fused_ws_kernel");
+}
+
+}  // namespace b2p

@@ -175,7 +175,7 @@ __device__ __forceinline__ void tc_teardown(const TcShared& sh, uint32_t tmem, b
 template <int MODE, bool RAGGED>
 __global__ void __launch_bounds__(kTcThreads, 1)
     syrk_tc_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0,
-                   int32_t* __restrict__ info) {
+                   int32_t* __restrict__ info, int jmax, int tiles_i, int tiles_j) {
   extern __shared__ unsigned char tc_raw[];
   const TcShared sh = tc_layout(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -195,14 +195,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     int ti = tg.ti, tj = tg.tj;
     if (!RAGGED) {
       const int q = blockIdx.x;
-      ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
-      while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
-      while (ti * (ti + 1) / 2 > q) --ti;
-      tj = q - ti * (ti + 1) / 2;
+      if (tiles_j >= tiles_i) {
+        ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+        while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
+        while (ti * (ti + 1) / 2 > q) --ti;
+        tj = q - ti * (ti + 1) / 2;
+      } else {
+        // Columns limited to the first tiles_j tile columns: column tj holds
+        // tiles ti = tj .. tiles_i-1.
+        int rem = q;
+        tj = 0;
+        while (rem >= tiles_i - tj) {
+          rem -= tiles_i - tj;
+          ++tj;
+        }
+        ti = tj + rem;
+      }
     }
     const int t0 = k0 + kTcK;
     const int i0 = t0 + ti * kTcTile, j0 = t0 + tj * kTcTile;
     const bool vec = (n & 3) == 0;
+    const int jlim = (RAGGED || jmax <= 0) ? n : jmax;
     const size_t moff = tg.off;
     const float* mat = l + moff;
     {
@@ -225,8 +238,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       float v[32];
       umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * ch), v);
       const int jc = j0 + 32 * ch;
-      if (i < n && jc <= i) {
-        if (vec && jc + 31 <= i) {
+      if (i < n && jc <= i && jc < jlim) {
+        if (vec && jc + 31 <= i && jc + 31 < jlim) {
 #pragma unroll
           for (int q4 = 0; q4 < 8; ++q4) {
             float4 c = *reinterpret_cast<const float4*>(crow + jc + 4 * q4);
@@ -239,7 +252,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         } else {
 #pragma unroll
           for (int e = 0; e < 32; ++e)
-            if (jc + e <= i) lrow[jc + e] = crow[jc + e] - v[e];
+            if (jc + e <= i && jc + e < jlim) lrow[jc + e] = crow[jc + e] - v[e];
         }
       }
     }
@@ -292,7 +305,7 @@ int T_tc(int n, int k0) {
 }
 
 int launch_syrk_tc(const float* csrc, float* l, const Sched& sch, bool ragged, int tiles, int k0, int mode,
-                   int32_t* info, cudaStream_t s) {
+                   int32_t* info, cudaStream_t s, int jmax) {
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
   const void* fn;
   int slot;
@@ -306,20 +319,27 @@ int launch_syrk_tc(const float* csrc, float* l, const Sched& sch, bool ragged, i
   }
   if (int st = ensure_smem_attr(fn, kTcSmemBytes, slot)) return st;
   dim3 grid;
+  int tiles_i = 0, tiles_j = 0;
   if (ragged) {
     if (sch.count <= 0) return B2P_OK;
     grid = dim3((unsigned)std::min<int64_t>(sch.count, 1 << 30), 1);
   } else {
     if (tiles <= 0 || sch.count <= 0) return B2P_OK;
-    grid = dim3(tiles * (tiles + 1) / 2, (unsigned)std::min<int64_t>(sch.count, 65535));
+    int tj = tiles;
+    if (jmax > 0) tj = std::min(tiles, (jmax - (k0 + kTcK) + kTcTile - 1) / kTcTile);
+    if (tj <= 0) return B2P_OK;
+    const int count = (tj >= tiles) ? tiles * (tiles + 1) / 2 : tj * tiles - tj * (tj - 1) / 2;
+    grid = dim3(count, (unsigned)std::min<int64_t>(sch.count, 65535));
+    tiles_i = tiles;
+    tiles_j = tj;
   }
   TraceScope ts(kKTrailTc, s);
   if (ragged) {
-    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
-    else syrk_tc_kernel<B2P_MODE_BF16X3, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
+    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info, jmax, tiles_i, tiles_j);
+    else syrk_tc_kernel<B2P_MODE_BF16X3, true><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info, jmax, tiles_i, tiles_j);
   } else {
-    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
-    else syrk_tc_kernel<B2P_MODE_BF16X3, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info);
+    if (tf32) syrk_tc_kernel<B2P_MODE_TF32, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info, jmax, tiles_i, tiles_j);
+    else syrk_tc_kernel<B2P_MODE_BF16X3, false><<<grid, kTcThreads, kTcSmemBytes, s>>>(csrc, l, sch, k0, info, jmax, tiles_i, tiles_j);
   }
   return check_launch("syrk_tc_kernel");
 }
