@@ -27,6 +27,8 @@ FLAG_FP64_DIAG = 0x100
 
 MODES = {"fp32": MODE_FP32, "tf32": MODE_TF32, "bf16x3": MODE_BF16X3, "fp8": MODE_FP8}
 
+PATHS = {"auto": 0, "blocked": 1, "fused": 2, "fused_ws": 3, "split": 4}
+
 # Every symbol the header declares, with (restype, argtypes).
 _c_i64 = ctypes.c_int64
 _c_sz = ctypes.c_size_t
@@ -39,6 +41,11 @@ SIGNATURES = {
     "b2p_potrf_batched": (
         ctypes.c_int,
         [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
+    ),
+    "b2p_potrf_path_workspace_size": (_c_sz, [_c_i64, _c_i64, ctypes.c_int, ctypes.c_int]),
+    "b2p_potrf_batched_path": (
+        ctypes.c_int,
+        [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
     ),
     "b2p_noalloc_scratch_bytes": (_c_sz, []),
     "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),

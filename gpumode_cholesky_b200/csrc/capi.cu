@@ -4,9 +4,11 @@
 // custom_kernel (submission.py:4101-4268) by routing on n alone:
 //   n <= 32    one warp per matrix            (potrf_warp32_kernel)
 //   n <= 128   one CTA per matrix, in smem    (potrf_cta128_kernel)
-//   n >  128   tensor modes, n <= 1024, n % 64 == 0:
-//                fused left-looking, one CTA per matrix (potrf_fused)
-//              otherwise blocked right-looking  (potrf_blocked)
+//   n >  128   tensor modes, n % 64 == 0 (choose_path):
+//                many CTAs per matrix when n > 1024 or the batch is too
+//                small to fill the GPU one CTA per matrix (potrf_split);
+//                else one CTA per matrix (potrf_fused / potrf_fused_ws);
+//              FP32 or any other n: blocked right-looking (potrf_blocked)
 // There is no CPU path and no vendor-library fallback.
 #include <cstdarg>
 #include <cstdio>
@@ -68,6 +70,37 @@ int ensure_smem_attr(const void* func, size_t bytes, int slot) {
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+static bool path_supported(int path, int64_t n, int mode) {
+  switch (path) {
+    case B2P_PATH_BLOCKED: return true;
+    case B2P_PATH_FUSED:
+    case B2P_PATH_FUSED_WS: return fused_supported(n, mode);
+    case B2P_PATH_SPLIT: return split_supported(n, mode);
+    default: return false;
+  }
+}
+
+// The n > 128 algorithm for (batch, n, mode).  Measured on B200 (BF16x3):
+// one CTA per matrix wins while the batch gives each SM most of a matrix
+// (60x1024: 932 us vs 1065 split; 16x512: 246 vs 254); a handful of large
+// matrices is faster spread over the GPU (4x1024: 511 vs 903).
+static int choose_path(int64_t batch, int64_t n, int mode) {
+  const int64_t sms = device_sms();
+  if (split_supported(n, mode) && (!fused_supported(n, mode) || (n >= 512 && batch * 16 <= sms)))
+    return B2P_PATH_SPLIT;
+  if (fused_supported(n, mode)) return batch > sms ? B2P_PATH_FUSED : B2P_PATH_FUSED_WS;
+  return B2P_PATH_BLOCKED;
+}
+
+static size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
+  switch (path) {
+    case B2P_PATH_FUSED:
+    case B2P_PATH_FUSED_WS: return fused_workspace_bytes(batch, n);
+    case B2P_PATH_SPLIT: return split_workspace_bytes(batch, n);
+    default: return blocked_workspace_bytes(batch, n, mode);
+  }
+}
+
 static int check_mode(int mode) {
   const int m = mode & B2P_MODE_MASK;
   if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG)) != 0)
@@ -98,15 +131,26 @@ const char* b2p_status_string(int status) {
 const char* b2p_last_error(void) { return g_msg; }
 
 size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode) {
-  if (batch <= 0 || n <= 128) return 0;
-  if (fused_supported(n, mode)) return fused_workspace_bytes(batch, n);
-  return blocked_workspace_bytes(batch, n, mode);
+  return b2p_potrf_path_workspace_size(batch, n, mode, B2P_PATH_AUTO);
+}
+
+size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int path) {
+  if (batch <= 0 || n <= 128 || check_mode(mode) != B2P_OK) return 0;
+  if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
+  if (!path_supported(path, n, mode)) return 0;
+  return path_workspace_bytes(path, batch, n, mode);
 }
 
 int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mode,
                       void* workspace, size_t workspace_bytes, int32_t* info, void* stream) {
+  return b2p_potrf_batched_path(a, l, batch, n, mode, B2P_PATH_AUTO, workspace, workspace_bytes, info, stream);
+}
+
+int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
+                           void* workspace, size_t workspace_bytes, int32_t* info, void* stream) {
   g_msg[0] = '\0';
   if (int st = check_mode(mode)) return st;
+  if (path < B2P_PATH_AUTO || path > B2P_PATH_SPLIT) return set_error(B2P_ERR_INVALID_ARG, "unknown path %d", path);
   if (batch < 0 || n < 0 || n > (1 << 20))
     return set_error(B2P_ERR_INVALID_ARG, "bad shape batch=%lld n=%lld", (long long)batch, (long long)n);
   if (batch == 0 || n == 0) return B2P_OK;
@@ -119,15 +163,15 @@ int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mo
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
-  if (fused_supported(n, mode)) {
-    // More matrices than SMs: two independent CTAs per SM hide each other's
-    // latency best; otherwise one warp-specialized CTA per matrix overlaps
-    // the next block column's update with the current panel.
-    if (batch > device_sms())
-      return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
-    return potrf_fused_ws(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+  if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
+  if (!path_supported(path, n, mode))
+    return set_error(B2P_ERR_UNSUPPORTED, "path %d does not support n=%lld mode 0x%x", path, (long long)n, mode);
+  switch (path) {
+    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
+    default: return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
   }
-  return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

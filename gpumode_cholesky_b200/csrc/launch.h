@@ -46,6 +46,13 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                    int32_t* info, cudaStream_t s);
 
+// Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
+// n > 128, tensor modes; two launches per 64-wide block column.
+bool split_supported(int64_t n, int mode);
+size_t split_workspace_bytes(int64_t batch, int64_t n);
+int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
+                int32_t* info, cudaStream_t s);
+
 // Batched tensor-core GEMM with structure hints (gemm_tc.cu):
 // C = alpha * op1(X) op2(Y) + beta * C per batch item.
 struct GemmArgs {
@@ -79,8 +86,8 @@ enum KernelId {
   kKPanel,
   kKTrail,
   kKTrailTc,
-  kKPanelTc,
-  kKSplit,
+  kKSplitStep,
+  kKSplitUpdate,
   kKRagged,
   kKBwdGemm,
   kKBwdTrsm,
@@ -123,6 +130,10 @@ enum SmemSlot {
   kSlotTcR1,
   kSlotFusedWs0,
   kSlotFusedWs1,
+  kSlotSplitU0,
+  kSlotSplitU1,
+  kSlotSplitS0,
+  kSlotSplitS1,
   kSlotCount
 };
 

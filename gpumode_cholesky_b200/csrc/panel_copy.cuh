@@ -1,0 +1,91 @@
+// Tensor-core copy of solved panels, shared by the left-looking kernels
+// (potrf_fused.cu, potrf_fused_ws.cu, potrf_split.cu).
+//
+// Every solved block column c (64 wide) of a matrix of order n = 64 N is
+// stored a second time in a workspace, already in the operand format of
+// tcgen05.mma: two regions per matrix (BF16 hi and lo of BF16x3, or the two
+// 32-column K-halves of TF32), each holding for column c the rows
+// 64(c+1)..n-1 (the only rows later updates read) as 128-byte K-major lines
+// in 8-row, 1024-byte 128B-swizzle atoms.  Rows of one column are contiguous,
+// so a 128-row operand tile is one 16 KB bulk copy per region, and the row
+// offset of column c is  64 (c (N-1) - c (c-1)/2)  rows from the region base.
+#pragma once
+
+#include "umma.cuh"
+
+namespace b2p {
+
+// Bytes of one region for a matrix of order n (n multiple of 64).
+__host__ __device__ inline size_t panel_copy_region_bytes(int n) {
+  const size_t N = (size_t)(n / 64);
+  return 4096 * N * (N - 1);
+}
+
+// Byte offset of global row r (r >= 64 (c+1)) of column c within a region.
+__device__ __forceinline__ size_t panel_copy_row_byte(int N, int c, int r) {
+  return (size_t)(64 * (c * (N - 1) - c * (c - 1) / 2) + r - 64 * (c + 1)) * 128;
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Store columns 8 tx .. 8 tx + 7 (values v) of global row r of column c.
+template <int MODE>
+__device__ __forceinline__ void panel_copy_store(uint8_t* w0, uint8_t* w1, int N, int c, int r, int tx,
+                                                 const float (&v)[8]) {
+  const size_t row = panel_copy_row_byte(N, c, r);
+  const int r8 = r & 7;
+  if (MODE == B2P_MODE_TF32) {
+    uint8_t* reg = (tx < 4) ? w0 : w1;
+    const int c0 = 2 * (tx & 3);
+    *reinterpret_cast<float4*>(reg + row + ((c0 ^ r8) << 4)) =
+        make_float4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
+    *reinterpret_cast<float4*>(reg + row + (((c0 + 1) ^ r8) << 4)) =
+        make_float4(tf32_rna(v[4]), tf32_rna(v[5]), tf32_rna(v[6]), tf32_rna(v[7]));
+  } else {
+    uint32_t h[4], lo[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      umma::split_bf16(v[2 * p], h0, l0);
+      umma::split_bf16(v[2 * p + 1], h1, l1);
+      h[p] = umma::pack_bf16(h0, h1);
+      lo[p] = umma::pack_bf16(l0, l1);
+    }
+    const size_t off = row + ((tx ^ r8) << 4);
+    *reinterpret_cast<uint4*>(w0 + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(w1 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
+// D (128 x 64 FP32 in TMEM) (+)= A B^T over one 64-wide column, from staged
+// copies: A = 128 rows at sa (region 0 at +0, region 1 at +16384), B = 64
+// rows at sb (region 0 at +0, region 1 at +8192).  One thread issues.
+template <int MODE>
+__device__ __forceinline__ void panel_copy_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
+  if (MODE == B2P_MODE_TF32) {
+    constexpr uint32_t idesc = umma::idesc_f32acc(2, 128, 64);
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
+      const uint32_t kb = (uint32_t)((s >> 2) * 8192 + (s & 3) * 32);
+      umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
+    }
+  } else {
+    constexpr uint32_t idesc = umma::idesc_f32acc(1, 128, 64);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const uint32_t o = (uint32_t)(s * 32);
+      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
+      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + 8192 + o);
+      umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
+      umma::mma_bf16(d, ah, bl, idesc, 1u);
+      umma::mma_bf16(d, ah, bh, idesc, 1u);
+    }
+  }
+}
+
+}  // namespace b2p

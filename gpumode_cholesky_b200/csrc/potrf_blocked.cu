@@ -53,7 +53,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // -------------------------------------------------------------------------
 // diag: factor + invert the 64x64 diagonal block of every matrix.
 template <bool RAGGED>
-__global__ void __launch_bounds__(kD64Threads, 4)
+__global__ void __launch_bounds__(kD64Threads, 3)
     diag_kernel(const float* __restrict__ src, float* __restrict__ l, Sched sch, int k0,
                 float* __restrict__ tws, int32_t* __restrict__ info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kD64Threads, 4)
         if (r < w && c < w) base[(size_t)r * n + c] = (c <= r) ? sm.S[r * kD64Ld + c] : 0.0f;
       }
     }
-    // T = inv(L_kk), row-major (the panel kernel transposes it on load).
+    // T^T (T = inv(L_kk)) as the engine leaves it: tws[m][c] = T[c][m].
     float* tb = tws + b * kNB * kNB;
 #pragma unroll
     for (int it = 0; it < 8; ++it) {
@@ -142,8 +142,12 @@ __global__ void __launch_bounds__(kD64Threads, 4)
       reinterpret_cast<float4*>(tb)[e4] = v;
     }
     if (info != nullptr && tid == 0) {
-      if (k0 == 0) info[tg.mat] = bad >= 0 ? bad + 1 : 0;
-      else if (bad >= 0 && info[tg.mat] == 0) info[tg.mat] = k0 + bad + 1;
+      if (bad == kDiagTimeout)
+        info[tg.mat] = -1;
+      else if (k0 == 0)
+        info[tg.mat] = bad >= 0 ? bad + 1 : 0;
+      else if (bad >= 0 && info[tg.mat] == 0)
+        info[tg.mat] = k0 + bad + 1;
     }
     __syncthreads();
   }
@@ -222,24 +226,16 @@ __global__ void __launch_bounds__(kGemmThreads)
     const int row0 = k0 + kNB + tg.ti * kTile;
     const size_t moff = tg.off;
     const float* tb = tws + tg.pos * kNB * kNB;
-    // Ts[m][c] = T[c][m]: consecutive threads take consecutive rows c of T,
-    // so the transposed stores are bank-conflict free.
+    // Ts[m][c] = T[c][m]: the diagonal kernel stored T^T row-major.
     {
       float4 tv[16];
 #pragma unroll
-      for (int it = 0; it < 16; ++it) {
-        const int e = tid + kGemmThreads * it;
-        tv[it] = __ldg(reinterpret_cast<const float4*>(tb) + (e & 63) * 16 + (e >> 6));
-      }
+      for (int it = 0; it < 16; ++it) tv[it] = __ldg(reinterpret_cast<const float4*>(tb) + tid + kGemmThreads * it);
       load_rows_t(src + moff, n, row0, k0, Ps);
 #pragma unroll
       for (int it = 0; it < 16; ++it) {
         const int e = tid + kGemmThreads * it;
-        const int c = e & 63, q = e >> 6;
-        Ts[(4 * q + 0) * kGemmLd + c] = tv[it].x;
-        Ts[(4 * q + 1) * kGemmLd + c] = tv[it].y;
-        Ts[(4 * q + 2) * kGemmLd + c] = tv[it].z;
-        Ts[(4 * q + 3) * kGemmLd + c] = tv[it].w;
+        *reinterpret_cast<float4*>(Ts + (e >> 4) * kGemmLd + (e & 15) * 4) = tv[it];
       }
     }
     __syncthreads();

@@ -29,6 +29,7 @@
 
 #include "diag64.cuh"
 #include "launch.h"
+#include "panel_copy.cuh"
 #include "umma.cuh"
 #include "xgemm.cuh"
 
@@ -38,7 +39,6 @@ constexpr int kFThreads = 256;
 constexpr int kFB = 64;     // block column width = K of each MMA chunk
 constexpr int kFM = 128;    // rows per M tile
 constexpr int kFPtLd = 132; // P^T in shared memory: [64][kFPtLd]
-constexpr int kFTtLd = 68;  // T^T in shared memory: [64][kFTtLd]
 constexpr uint32_t kFPolls = 1u << 24;
 
 // Phase-1 staging: 2 stages x (A: 2 regions x 16 KB, B: 2 regions x 8 KB).
@@ -46,87 +46,13 @@ constexpr uint32_t kFStageA = 32768;
 constexpr uint32_t kFStageB = 16384;
 constexpr uint32_t kFStage = kFStageA + kFStageB;
 constexpr uint32_t kFStaging = 2 * kFStage;
-// Phase-2 layout in the same region.
+// Phase-2 layout in the same region.  The workspace holds the panel copies
+// (panel_copy.cuh).
 constexpr uint32_t kFPtOff = ((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u;
-constexpr uint32_t kFTtOff = kFPtOff + 64 * kFPtLd * 4;
-constexpr uint32_t kFPhase2 = kFTtOff + 64 * kFTtLd * 4;
+constexpr uint32_t kFPhase2 = kFPtOff + 64 * kFPtLd * 4;
 constexpr uint32_t kFUnion = kFStaging > kFPhase2 ? kFStaging : kFPhase2;
 constexpr uint32_t kFSmemBytes = kFUnion + 128 + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
-
-// Workspace: per matrix two regions (BF16 hi / lo, or TF32 K-halves) of
-// 4096 * N * (N-1) bytes, N = n / 64.  Column c keeps rows 64(c+1)..n-1 (the
-// only rows later updates read), 128 bytes per row, in 8-row 1024-byte
-// swizzle atoms.
-__host__ __device__ inline size_t fused_region_bytes(int n) {
-  const size_t N = (size_t)(n / kFB);
-  return 4096 * N * (N - 1);
-}
-__device__ __forceinline__ size_t fused_row_byte(int N, int c, int r) {
-  return (size_t)(64 * (c * (N - 1) - c * (c - 1) / 2) + r - 64 * (c + 1)) * 128;
-}
-
-template <int MODE>
-__device__ __forceinline__ void fused_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
-  if (MODE == B2P_MODE_TF32) {
-    constexpr uint32_t idesc = umma::idesc_f32acc(2, kFM, kFB);
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
-      const uint32_t kb = (uint32_t)((s >> 2) * 8192 + (s & 3) * 32);
-      umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
-    }
-  } else {
-    constexpr uint32_t idesc = umma::idesc_f32acc(1, kFM, kFB);
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const uint32_t o = (uint32_t)(s * 32);
-      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
-      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + 8192 + o);
-      umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
-      umma::mma_bf16(d, ah, bl, idesc, 1u);
-      umma::mma_bf16(d, ah, bh, idesc, 1u);
-    }
-  }
-}
-
-__device__ __forceinline__ float fused_round_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
-// Tensor-core copy of 8 consecutive values (columns 8*tx..8*tx+7) of global
-// row r of block column c.
-template <int MODE>
-__device__ __forceinline__ void fused_store_ws(uint8_t* w0, uint8_t* w1, int N, int c, int r, int tx,
-                                               const float (&v)[8]) {
-  const size_t row = fused_row_byte(N, c, r);
-  const int r8 = r & 7;
-  if (MODE == B2P_MODE_TF32) {
-    uint8_t* reg = (tx < 4) ? w0 : w1;
-    const int c0 = 2 * (tx & 3);
-    const float4 lo = make_float4(fused_round_tf32(v[0]), fused_round_tf32(v[1]), fused_round_tf32(v[2]),
-                                  fused_round_tf32(v[3]));
-    const float4 hi = make_float4(fused_round_tf32(v[4]), fused_round_tf32(v[5]), fused_round_tf32(v[6]),
-                                  fused_round_tf32(v[7]));
-    *reinterpret_cast<float4*>(reg + row + ((c0 ^ r8) << 4)) = lo;
-    *reinterpret_cast<float4*>(reg + row + (((c0 + 1) ^ r8) << 4)) = hi;
-  } else {
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      __nv_bfloat16 h0, l0, h1, l1;
-      umma::split_bf16(v[2 * p], h0, l0);
-      umma::split_bf16(v[2 * p + 1], h1, l1);
-      h[p] = umma::pack_bf16(h0, h1);
-      l[p] = umma::pack_bf16(l0, l1);
-    }
-    const size_t off = row + ((tx ^ r8) << 4);
-    *reinterpret_cast<uint4*>(w0 + off) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(w1 + off) = make_uint4(l[0], l[1], l[2], l[3]);
-  }
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
@@ -136,7 +62,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
   float* PtT = reinterpret_cast<float*>(sm + kFPtOff);
-  float* TT = reinterpret_cast<float*>(sm + kFTtOff);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kFUnion);  // [2]
   uint64_t* empty = full + 2;                                   // [2]
   uint64_t* done = full + 4;                                    // [1]
@@ -146,7 +71,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kFB;
-  const size_t rbytes = fused_region_bytes(n);
+  const size_t rbytes = panel_copy_region_bytes(n);
 
   if (tid == 0) *flag = 0;
   if (warp == 0) {
@@ -187,8 +112,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
             const int mt = i / k, kc = i - (i / k) * k;
             const int r0 = k0 + mt * kFM;
             const uint32_t abytes = (uint32_t)min(kFM, n - r0) * 128u;
-            const size_t aoff = fused_row_byte(N, kc, r0);
-            const size_t boff = fused_row_byte(N, kc, k0);
+            const size_t aoff = panel_copy_row_byte(N, kc, r0);
+            const size_t boff = panel_copy_row_byte(N, kc, k0);
             uint8_t* st = sm + s * kFStage;
             umma::mbar_arrive_expect_tx(full + s, 2 * abytes + 2 * 8192u);
             umma::bulk_g2s(st, W0 + aoff, abytes, full + s);
@@ -215,7 +140,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
             umma::fence_after_sync();
             const int mt = i / k, kc = i - (i / k) * k;
             const uint32_t st = umma::smem_u32(sm + s * kFStage);
-            fused_mmas<MODE>(tmem + (uint32_t)(kFB * mt), st, st + kFStageA, kc > 0);
+            panel_copy_mmas<MODE>(tmem + (uint32_t)(kFB * mt), st, st + kFStageA, kc > 0);
             umma::mma_commit(empty + s);
             ++n_empty[s];
             if (i + 2 < iters) {
@@ -296,12 +221,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
         umma::fence_before_sync();
         __syncthreads();
         if (mt == 0) {
+          // L_kk and T^T (T = L_kk^{-1}, in dg.T) from the pipelined engine.
           const int bad = diag64_factor_invert(dg);
-          if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
-          for (int e = tid; e < 64 * 64; e += kFThreads) {
-            const int m = e >> 6, c = e & 63;
-            TT[m * kFTtLd + c] = dg.T[c * kD64Ld + m];
+          if (bad == kDiagTimeout) {
+            ok = false;
+            break;
           }
+          if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
           for (int e = tid; e < 64 * 16; e += kFThreads) {
             const int r = e >> 4, c = (e & 15) * 4;
@@ -320,7 +246,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
         }
         // X = P T^T for the rows below the diagonal block (triangle skipped),
         // then L and the tensor-core copy from X^T.
-        xgemm_tri_inplace(PtT, kFPtLd, TT, kFTtLd, CtaBarrier());
+        xgemm_tri_inplace(PtT, kFPtLd, dg.T, kD64Ld, CtaBarrier());
         for (int item = tid; item < kFM * 8; item += kFThreads) {
           const int rl = item & (kFM - 1), c = item >> 7;
           if (rl >= vr || (mt == 0 && rl < 64)) continue;
@@ -331,10 +257,11 @@ __global__ void __launch_bounds__(kFThreads, 2)
           float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * c);
           dst[0] = make_float4(v[0], v[1], v[2], v[3]);
           dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-          if (k + 1 < N) fused_store_ws<MODE>(W0, W1, N, k, rg, c, v);
+          if (k + 1 < N) panel_copy_store<MODE>(W0, W1, N, k, rg, c, v);
         }
         __syncthreads();
       }
+      if (!ok) break;
       // Workspace and shared-memory writes above must be ordered before the
       // next step's bulk copies and tensor-core reads (async proxy).
       umma::fence_proxy_async_all();
@@ -355,7 +282,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
 // The workspace pointer is rounded up to 1024 bytes inside, hence the slack.
 size_t fused_workspace_bytes(int64_t batch, int64_t n) {
-  return (size_t)batch * 2 * fused_region_bytes((int)n) + 1024;
+  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 1024;
 }
 
 bool fused_supported(int64_t n, int mode) {

@@ -29,6 +29,7 @@
 
 #include "diag64.cuh"
 #include "launch.h"
+#include "panel_copy.cuh"
 #include "umma.cuh"
 #include "xgemm.cuh"
 
@@ -39,7 +40,6 @@ constexpr int kWThreads = kWConsumers + 32;
 constexpr int kWB = 64;
 constexpr int kWM = 128;
 constexpr int kWPtLd = 132;
-constexpr int kWTtLd = 68;
 constexpr uint32_t kWPolls = 1u << 24;
 constexpr uint32_t kWTmemCols = 512;
 
@@ -47,21 +47,10 @@ constexpr uint32_t kWStageA = 32768;
 constexpr uint32_t kWStage = kWStageA + 16384;
 constexpr uint32_t kWDiagOff = 2 * kWStage;
 constexpr uint32_t kWPtOff = kWDiagOff + (((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u);
-constexpr uint32_t kWTtOff = kWPtOff + 64 * kWPtLd * 4;
-constexpr uint32_t kWBarOff = kWTtOff + 64 * kWTtLd * 4;
+constexpr uint32_t kWBarOff = kWPtOff + 64 * kWPtLd * 4;
 constexpr uint32_t kWSmemBytes = kWBarOff + 256 + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
-
-__device__ __forceinline__ size_t ws_row_byte(int N, int c, int r) {
-  return (size_t)(64 * (c * (N - 1) - c * (c - 1) / 2) + r - 64 * (c + 1)) * 128;
-}
-
-__device__ __forceinline__ float ws_round_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(mbar)) : "memory");
@@ -74,58 +63,6 @@ __device__ __forceinline__ bool ws_wait(uint64_t* mbar, uint32_t parity, volatil
     if ((i & 255u) == 255u && *flag) return false;
   }
   return false;
-}
-
-template <int MODE>
-__device__ __forceinline__ void ws_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
-  if (MODE == B2P_MODE_TF32) {
-    constexpr uint32_t idesc = umma::idesc_f32acc(2, kWM, kWB);
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
-      const uint32_t kb = (uint32_t)((s >> 2) * 8192 + (s & 3) * 32);
-      umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
-    }
-  } else {
-    constexpr uint32_t idesc = umma::idesc_f32acc(1, kWM, kWB);
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const uint32_t o = (uint32_t)(s * 32);
-      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
-      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + 8192 + o);
-      umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
-      umma::mma_bf16(d, ah, bl, idesc, 1u);
-      umma::mma_bf16(d, ah, bh, idesc, 1u);
-    }
-  }
-}
-
-template <int MODE>
-__device__ __forceinline__ void ws_store_copy(uint8_t* w0, uint8_t* w1, int N, int c, int r, int tx,
-                                              const float (&v)[8]) {
-  const size_t row = ws_row_byte(N, c, r);
-  const int r8 = r & 7;
-  if (MODE == B2P_MODE_TF32) {
-    uint8_t* reg = (tx < 4) ? w0 : w1;
-    const int c0 = 2 * (tx & 3);
-    *reinterpret_cast<float4*>(reg + row + ((c0 ^ r8) << 4)) =
-        make_float4(ws_round_tf32(v[0]), ws_round_tf32(v[1]), ws_round_tf32(v[2]), ws_round_tf32(v[3]));
-    *reinterpret_cast<float4*>(reg + row + (((c0 + 1) ^ r8) << 4)) =
-        make_float4(ws_round_tf32(v[4]), ws_round_tf32(v[5]), ws_round_tf32(v[6]), ws_round_tf32(v[7]));
-  } else {
-    uint32_t h[4], lo[4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      __nv_bfloat16 h0, l0, h1, l1;
-      umma::split_bf16(v[2 * p], h0, l0);
-      umma::split_bf16(v[2 * p + 1], h1, l1);
-      h[p] = umma::pack_bf16(h0, h1);
-      lo[p] = umma::pack_bf16(l0, l1);
-    }
-    const size_t off = row + ((tx ^ r8) << 4);
-    *reinterpret_cast<uint4*>(w0 + off) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(w1 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-  }
 }
 
 struct WsBars {
@@ -145,7 +82,7 @@ struct WsBars {
 template <int MODE>
 __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t batch, int n, uint32_t tmem) {
   const int N = n / kWB;
-  const size_t rbytes = (size_t)4096 * N * (N - 1);
+  const size_t rbytes = panel_copy_region_bytes(n);
   uint32_t n_load[2] = {0u, 0u}, n_empty[2] = {0u, 0u};
   int writes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t biter = 0;
@@ -187,8 +124,8 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
         if (kc == k - 1 && !deps_ready(mt, true)) return false;
         const int r0 = k0 + mt * kWM;
         const uint32_t abytes = (uint32_t)min(kWM, n - r0) * 128u;
-        const size_t aoff = ws_row_byte(N, kc, r0);
-        const size_t boff = ws_row_byte(N, kc, k0);
+        const size_t aoff = panel_copy_row_byte(N, kc, r0);
+        const size_t boff = panel_copy_row_byte(N, kc, k0);
         uint8_t* st = sm + s * kWStage;
         umma::mbar_arrive_expect_tx(br.full + s, 2 * abytes + 2 * 8192u);
         umma::bulk_g2s(st, W0 + aoff, abytes, br.full + s);
@@ -223,7 +160,7 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
         }
         umma::fence_after_sync();
         const uint32_t st = umma::smem_u32(sm + s * kWStage);
-        ws_mmas<MODE>(tmem + (uint32_t)(kWB * mt), st, st + kWStageA, kc > 0);
+        panel_copy_mmas<MODE>(tmem + (uint32_t)(kWB * mt), st, st + kWStageA, kc > 0);
         umma::mma_commit(br.empty + s);
         ++n_empty[s];
         if (kc == k - 1) {
@@ -254,10 +191,9 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
-  float* TT = reinterpret_cast<float*>(sm + kWTtOff);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kWB;
-  const size_t rbytes = (size_t)4096 * N * (N - 1);
+  const size_t rbytes = panel_copy_region_bytes(n);
   uint32_t ready_par = 0u;  // bit t: parity of the next acc_ready phase of tile t
   for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
     const float* A = a + (size_t)b * n * n;
@@ -320,14 +256,14 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           }
         }
         cbar();
-        // (b) diagonal block: factor, invert, T^T, L_kk, zero strip.
+        // (b) diagonal block: L_kk and T^T (pipelined engine), zero strip.
         if (mt == 0) {
           const int bad = diag64_factor_invert(dg, cbar);
-          if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
-          for (int e = tid; e < 64 * 64; e += kWConsumers) {
-            const int m = e >> 6, c = e & 63;
-            TT[m * kWTtLd + c] = dg.T[c * kD64Ld + m];
+          if (bad == kDiagTimeout) {
+            failed = true;
+            if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
+          if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
           for (int e = tid; e < 64 * 16; e += kWConsumers) {
             const int r = e >> 4, c = (e & 15) * 4;
             const float* srow = dg.S + r * kD64Ld + c;
@@ -343,7 +279,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           cbar();
         }
         // (c) X = P T^T (triangle skipped), then L and the tensor-core copy from X^T.
-        xgemm_tri_inplace(PtT, kWPtLd, TT, kWTtLd, cbar);
+        xgemm_tri_inplace(PtT, kWPtLd, dg.T, kD64Ld, cbar);
         for (int item = tid; item < kWM * 8; item += kWConsumers) {
           const int rl = item & (kWM - 1), c = item >> 7;
           if (rl >= vr || (mt == 0 && rl < 64)) continue;
@@ -354,7 +290,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * c);
           dst[0] = make_float4(v[0], v[1], v[2], v[3]);
           dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-          if (k + 1 < N) ws_store_copy<MODE>(W0, W1, N, k, rg, c, v);
+          if (k + 1 < N) panel_copy_store<MODE>(W0, W1, N, k, rg, c, v);
         }
         // Publish this tile's panel rows to the producer's bulk copies.
         umma::fence_proxy_async_all();

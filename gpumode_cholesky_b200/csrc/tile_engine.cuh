@@ -29,6 +29,14 @@ constexpr int kLtLd = 36;
 // identity padding.  On return x holds L (lower part valid, upper part is
 // don't-care) and inv_pivot holds 1/L[lane][lane].  Returns the first local
 // pivot index that was not positive, or -1.  All 32 lanes must call.
+//
+// Step k takes the pivot d = x[k] of lane k and, in the same round of
+// shuffles, lane k+1's unscaled column-k value e; every lane then forms
+// L[k+1][k] = e / sqrt(d) itself and updates its column k+1 at once, so the
+// next pivot depends only on shuffles and registers.  The rest of the rank-1
+// update (columns k+2..31) goes through a double-buffered shared-memory copy
+// of column k, off that critical chain.  The arithmetic is the same as the
+// textbook right-looking update, value for value.
 __device__ __forceinline__ int warp_factor32(float (&x)[32], int lane, int w, float* colbuf,
                                              float& inv_pivot) {
   int bad = -1;
@@ -37,22 +45,26 @@ __device__ __forceinline__ int warp_factor32(float (&x)[32], int lane, int w, fl
   for (int k = 0; k < 32; ++k) {
     if (k < w) {  // warp-uniform
       const float d = __shfl_sync(kFullMask, x[k], k);
+      const float e = (k + 1 < 32) ? __shfl_sync(kFullMask, x[k], k + 1) : 0.0f;
       if (bad < 0 && pivot_bad(d)) bad = k;
       const float y = rsqrt_refined(d);
       if (lane == k) inv_pivot = y;
       x[k] = (lane == k) ? d * y : x[k] * y;
-      float* cb = colbuf + (k & 1) * 32;
-      cb[lane] = x[k];
-      __syncwarp();
-      // x[j] -= L[lane][k] * L[j][k] for j > k (upper part is don't-care).
+      if (k + 1 < 32) x[k + 1] = fmaf(-x[k], e * y, x[k + 1]);
+      if (k + 2 < 32) {
+        float* cb = colbuf + (k & 1) * 32;
+        cb[lane] = x[k];
+        __syncwarp();
+        // x[j] -= L[lane][k] * L[j][k] for j > k + 1 (upper part is don't-care).
 #pragma unroll
-      for (int j4 = (k + 1) / 4; j4 < 8; ++j4) {
-        const float4 c = reinterpret_cast<const float4*>(cb)[j4];
-        const float cv[4] = {c.x, c.y, c.z, c.w};
+        for (int j4 = (k + 2) / 4; j4 < 8; ++j4) {
+          const float4 c = reinterpret_cast<const float4*>(cb)[j4];
+          const float cv[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int j = 4 * j4 + e;
-          if (j > k) x[j] = fmaf(-x[k], cv[e], x[j]);
+          for (int q = 0; q < 4; ++q) {
+            const int j = 4 * j4 + q;
+            if (j > k + 1) x[j] = fmaf(-x[k], cv[q], x[j]);
+          }
         }
       }
     }

@@ -68,14 +68,19 @@ def cholesky(
     mode: str | int | None = None,
     out: torch.Tensor | None = None,
     info: torch.Tensor | None = None,
+    path: str = "auto",
 ) -> torch.Tensor:
     """Factor a batch of SPD matrices: returns L with A = L L^T.
 
     ``mode`` selects the trailing-update arithmetic ("fp32", "tf32",
     "bf16x3", "fp8", optionally suffixed "+fp64diag").  ``info`` may be an
     int32 CUDA tensor of shape (batch,) that receives 0 or the 1-based index
-    of the first non-positive pivot.
+    of the first non-positive pivot.  ``path`` forces the algorithm for
+    n > 128 ("blocked", "fused", "fused_ws", "split"; default "auto").
     """
+    if path not in _lib.PATHS:
+        raise ValueError(f"unknown path {path!r}; expected one of {sorted(_lib.PATHS)}")
+    pcode = _lib.PATHS[path]
     _check_input(a)
     a = a.contiguous()
     batch, n, _ = a.shape
@@ -86,17 +91,17 @@ def cholesky(
         raise ValueError("out must be a contiguous float32 tensor shaped like the input, on the same device")
     lib = _lib.load()
     with torch.cuda.device(a.device):
-        ws_bytes = lib.b2p_potrf_workspace_size(batch, n, code)
+        ws_bytes = lib.b2p_potrf_path_workspace_size(batch, n, code, pcode)
         ws_ptr = workspace(a.device, ws_bytes).data_ptr() if ws_bytes else None
         info_ptr = None
         if info is not None:
             if info.dtype != torch.int32 or info.numel() < batch or not info.is_cuda:
                 raise ValueError("info must be an int32 CUDA tensor with at least batch elements")
             info_ptr = info.data_ptr()
-        st = lib.b2p_potrf_batched(
-            a.data_ptr(), out.data_ptr(), batch, n, code, ws_ptr, ws_bytes, info_ptr, _stream_ptr(a.device)
+        st = lib.b2p_potrf_batched_path(
+            a.data_ptr(), out.data_ptr(), batch, n, code, pcode, ws_ptr, ws_bytes, info_ptr, _stream_ptr(a.device)
         )
-    _lib.check(st, "b2p_potrf_batched")
+    _lib.check(st, "b2p_potrf_batched_path")
     return out
 
 

@@ -87,6 +87,31 @@ B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n
                       void* stream);
 
 /*
+ * Algorithm selection for n > 128.  b2p_potrf_batched picks one from
+ * (batch, n, mode) (B2P_PATH_AUTO); the _path variants force one, for tests
+ * that cover every kernel family and for tuning:
+ *   B2P_PATH_BLOCKED   right-looking, one launch per kernel and block column
+ *                      (any n > 128, every mode);
+ *   B2P_PATH_FUSED     left-looking, one CTA per matrix, two per SM
+ *                      (tensor modes, n % 64 == 0, n <= 1024);
+ *   B2P_PATH_FUSED_WS  the same, warp-specialized, one CTA per SM;
+ *   B2P_PATH_SPLIT     left-looking over many CTAs per matrix, two launches
+ *                      per block column (tensor modes, n % 64 == 0).
+ * A path that does not support (n, mode) returns B2P_ERR_UNSUPPORTED, and
+ * its workspace query returns 0.  n <= 128 ignores the path.  No
+ * counterpart exists in the reference (its dispatcher hard-codes one route
+ * per benchmark shape, submission.py:4111-4268).
+ */
+#define B2P_PATH_AUTO 0
+#define B2P_PATH_BLOCKED 1
+#define B2P_PATH_FUSED 2
+#define B2P_PATH_FUSED_WS 3
+#define B2P_PATH_SPLIT 4
+B2P_API size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int path);
+B2P_API int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
+                                   void* workspace, size_t workspace_bytes, int32_t* info, void* stream);
+
+/*
  * Allocation-free variant of b2p_potrf_batched for callers that cannot
  * allocate device memory (code inside an allocator-free region, a plugin
  * whose host owns every device allocation, a serving process that forbids

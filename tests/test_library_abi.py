@@ -73,6 +73,21 @@ def test_workspace_sizes_are_host_only():
     assert lib.b2p_potrf_workspace_size(0, 512, 0) == 0
 
 
+def test_path_workspace_sizes():
+    """Forced paths: a path that cannot run (n, mode) reports 0 bytes."""
+    lib = _lib.load()
+    p = _lib.PATHS
+    bf = _lib.MODE_BF16X3
+    assert lib.b2p_potrf_path_workspace_size(4, 2048, bf, p["fused"]) == 0  # one CTA per matrix stops at 1024
+    assert lib.b2p_potrf_path_workspace_size(4, 200, bf, p["split"]) == 0  # needs n % 64 == 0
+    assert lib.b2p_potrf_path_workspace_size(4, 512, _lib.MODE_FP32, p["split"]) == 0  # tensor modes only
+    assert lib.b2p_potrf_path_workspace_size(4, 512, bf, p["blocked"]) > 0
+    assert lib.b2p_potrf_path_workspace_size(4, 512, bf, p["split"]) > lib.b2p_potrf_path_workspace_size(4, 512, bf, p["fused"])
+    assert lib.b2p_potrf_path_workspace_size(4, 64, bf, p["split"]) == 0  # n <= 128 needs none
+    # an unknown path is rejected before any device work
+    assert lib.b2p_potrf_batched_path(ctypes.c_void_p(4096), ctypes.c_void_p(1 << 30), 1, 512, bf, 9, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+
+
 def test_error_raises_python_exception():
     with pytest.raises(_lib.PotrfError) as ei:
         _lib.check(_lib.B2P_ERR_UNSUPPORTED, "call")
