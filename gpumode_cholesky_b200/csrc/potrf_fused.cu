@@ -51,7 +51,9 @@ constexpr uint32_t kFStaging = 2 * kFStage;
 constexpr uint32_t kFPtOff = ((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u;
 constexpr uint32_t kFPhase2 = kFPtOff + 64 * kFPtLd * 4;
 constexpr uint32_t kFUnion = kFStaging > kFPhase2 ? kFStaging : kFPhase2;
-constexpr uint32_t kFSmemBytes = kFUnion + 128 + 1024;
+constexpr uint32_t kFZeroOff = kFUnion + 128;  // zeros, source of the strip's bulk stores
+constexpr uint32_t kFZeroBytes = 4096;           // >= 4 (n - 64) bytes for n <= 1024
+constexpr uint32_t kFSmemBytes = kFZeroOff + kFZeroBytes + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
 
 template <int MODE>
@@ -74,6 +76,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
   const size_t rbytes = panel_copy_region_bytes(n);
 
   if (tid == 0) *flag = 0;
+  for (uint32_t e = tid; e < kFZeroBytes / 16; e += kFThreads)
+    reinterpret_cast<float4*>(sm + kFZeroOff)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  umma::fence_proxy_async_smem();  // the zeros are read by bulk stores
   if (warp == 0) {
     umma::tmem_alloc(tslot, tmem_cols);
     umma::tmem_relinquish();
@@ -236,11 +241,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
                                    c + 3 <= r ? srow[3] : 0.f);
             *reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + c) = v;
           }
-          // Zero strip right of the diagonal block.
-          const int s4 = (n - k0 - kFB) >> 2;
-          for (int e = tid; e < 64 * s4; e += kFThreads) {
-            const int r = e / s4, q = e - (e / s4) * s4;
-            reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + kFB)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+          // Zero strip right of the diagonal block: one bulk store per row from
+          // the zero buffer, issued by one thread and left to run.
+          const uint32_t strip = 4u * (uint32_t)(n - k0 - kFB);
+          if (tid == 0 && strip > 0) {
+            for (int r = 0; r < 64; ++r)
+              umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kFB, sm + kFZeroOff, strip);
+            umma::bulk_commit();
           }
           __syncthreads();
         }
@@ -271,6 +278,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
   }
+  // The strip's bulk stores read the zero buffer until they complete.
+  if (tid == 0) umma::bulk_wait_all();
   // Release TMEM after a last bounded chance for outstanding MMAs.
   if (!ok) {
     umma::mbar_wait_bounded(done, ph_done, kFPolls);

@@ -47,7 +47,9 @@ constexpr uint32_t kWStageA = 32768;
 constexpr uint32_t kWStage = kWStageA + 16384;
 constexpr uint32_t kWDiagOff = 2 * kWStage;
 constexpr uint32_t kWPtOff = kWDiagOff + (((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u);
-constexpr uint32_t kWBarOff = kWPtOff + 64 * kWPtLd * 4;
+constexpr uint32_t kWZeroOff = kWPtOff + 64 * kWPtLd * 4;  // zeros, source of the strip's bulk stores
+constexpr uint32_t kWZeroBytes = 4096;                    // >= 4 (n - 64) bytes for n <= 1024
+constexpr uint32_t kWBarOff = kWZeroOff + kWZeroBytes;
 constexpr uint32_t kWSmemBytes = kWBarOff + 256 + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
@@ -191,6 +193,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
+  const float* zeros = reinterpret_cast<const float*>(sm + kWZeroOff);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
@@ -271,37 +274,48 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
                                          c + 2 <= r ? srow[2] : 0.f, c + 3 <= r ? srow[3] : 0.f);
             *reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + c) = v;
           }
-          const int s4 = (n - k0 - kWB) >> 2;
-          for (int e = tid; e < 64 * s4; e += kWConsumers) {
-            const int r = e / s4, q = e - (e / s4) * s4;
-            reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + kWB)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+          // Zero strip right of the diagonal block: one bulk store per row from
+          // the zero buffer, issued by one thread and left to run.
+          const uint32_t strip = 4u * (uint32_t)(n - k0 - kWB);
+          if (tid == 0 && strip > 0) {
+            for (int r = 0; r < 64; ++r) umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kWB, zeros, strip);
+            umma::bulk_commit();
           }
           cbar();
         }
         // (c) X = P T^T (triangle skipped), then L and the tensor-core copy from X^T.
         xgemm_tri_inplace(PtT, kWPtLd, dg.T, kD64Ld, cbar);
-        for (int item = tid; item < kWM * 8; item += kWConsumers) {
-          const int rl = item & (kWM - 1), c = item >> 7;
-          if (rl >= vr || (mt == 0 && rl < 64)) continue;
-          float v[8];
+        // Output: first the tensor-core copy, published to the producer's bulk
+        // copies (the proxy fence then covers only these stores), then L.
+        float v[4][8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) v[j] = PtT[(8 * c + j) * kWPtLd + rl];
-          const int rg = r0 + rl;
-          float4* dst = reinterpret_cast<float4*>(L + (size_t)rg * n + k0 + 8 * c);
-          dst[0] = make_float4(v[0], v[1], v[2], v[3]);
-          dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-          if (k + 1 < N) panel_copy_store<MODE>(W0, W1, N, k, rg, c, v);
+        for (int it = 0; it < 4; ++it) {
+          const int item = tid + kWConsumers * it;
+          const int rl = item & (kWM - 1), c = item >> 7;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v[it][j] = PtT[(8 * c + j) * kWPtLd + rl];
+          if (k + 1 < N && rl < vr && !(mt == 0 && rl < 64)) panel_copy_store<MODE>(W0, W1, N, k, r0 + rl, c, v[it]);
         }
-        // Publish this tile's panel rows to the producer's bulk copies.
         umma::fence_proxy_async_all();
         __syncwarp();
         if (lane == 0) mbar_arrive(br.tile_ready + mt);
+#pragma unroll
+        for (int it = 0; it < 4; ++it) {
+          const int item = tid + kWConsumers * it;
+          const int rl = item & (kWM - 1), c = item >> 7;
+          if (rl >= vr || (mt == 0 && rl < 64)) continue;
+          float4* dst = reinterpret_cast<float4*>(L + (size_t)(r0 + rl) * n + k0 + 8 * c);
+          dst[0] = make_float4(v[it][0], v[it][1], v[it][2], v[it][3]);
+          dst[1] = make_float4(v[it][4], v[it][5], v[it][6], v[it][7]);
+        }
         cbar();
       }
     }
     if (tid == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
     if (failed) break;
   }
+  // The strip's bulk stores read the zero buffer until they complete.
+  if (tid == 0) umma::bulk_wait_all();
 }
 
 template <int MODE>
@@ -323,6 +337,10 @@ __global__ void __launch_bounds__(kWThreads, 1)
   br.badp = reinterpret_cast<int*>(bars + 30) + 1;
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) *br.flag = 0;
+  for (uint32_t e = tid; e < kWZeroBytes / 16; e += kWThreads)
+    reinterpret_cast<float4*>(sm + kWZeroOff)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  // The zeros are read by the async proxy (bulk stores).
+  umma::fence_proxy_async_smem();
   if (warp == 0) {
     umma::tmem_alloc(br.tslot, kWTmemCols);
     umma::tmem_relinquish();
