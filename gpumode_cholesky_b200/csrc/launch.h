@@ -130,6 +130,8 @@ enum SmemSlot {
   kSlotTcR1,
   kSlotFusedWs0,
   kSlotFusedWs1,
+  kSlotFusedWs2,
+  kSlotFusedWs3,
   kSlotSplitU0,
   kSlotSplitU1,
   kSlotSplitS0,

@@ -11,7 +11,16 @@
 //   warps 0-7 (consumers)  per tile: wait `acc_ready`, read D from TMEM
 //        (then arrive `acc_free`), P = A - D, factor + invert the diagonal
 //        block (tile 0), X = P T^T in FP32, write L and the tensor-core copy
-//        of X, then arrive `tile_ready`.
+//        of X, then publish the tile's completion count.
+//
+// Small batches run as clusters of two CTAs per matrix (CL = 2): rank 0 takes
+// the even row tiles of every block column (tile 0 holds the diagonal block),
+// rank 1 the odd ones, and rank 1 also accumulates its own copy of tile 0 to
+// factor the diagonal block redundantly, so the two CTAs share only panel
+// copies in global memory.  A finished tile is announced to both CTAs'
+// producers through per-tile completion counters (release stores at cluster
+// scope, bounded acquire polls), which cannot alias the way an mbarrier
+// phase can when its waiter falls behind a CTA it does not pace.
 //
 // Ordering rules (every mbarrier is waited at most one phase behind):
 //   * MMA write #w into TMEM tile t waits for consumer read #(w-1) of t;
@@ -67,12 +76,41 @@ __device__ __forceinline__ bool ws_wait(uint64_t* mbar, uint32_t parity, volatil
   return false;
 }
 
+__device__ __forceinline__ int ld_acquire_cluster(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cluster.shared::cta.b32 %0, [%1];" : "=r"(v) : "r"(umma::smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cluster(const int* local, uint32_t rank, int v) {
+  asm volatile("st.release.cluster.shared::cluster.b32 [%0], %1;" ::"r"(umma::cluster_addr(local, rank)), "r"(v)
+               : "memory");
+}
+// Bounded wait until the completion counter *p reaches `target`.
+__device__ __forceinline__ bool ws_wait_count(const int* p, int target, volatile int* flag, bool block) {
+  for (uint32_t i = 0; i < (block ? kWPolls : 1u); ++i) {
+    if (ld_acquire_cluster(p) >= target) return true;
+    if ((i & 255u) == 255u && *flag) return false;
+  }
+  return false;
+}
+
+// Row tiles of a block column (mt_n of them) that CTA `rank` of a CL-CTA
+// cluster accumulates: j-th tile and count.
+template <int CL>
+__device__ __forceinline__ int ws_tile_count(int mt_n, int rank) {
+  return CL == 1 ? mt_n : (rank == 0 ? (mt_n + 1) / 2 : 1 + mt_n / 2);
+}
+template <int CL>
+__device__ __forceinline__ int ws_tile_of(int j, int rank) {
+  return CL == 1 ? j : (rank == 0 ? 2 * j : (j == 0 ? 0 : 2 * j - 1));
+}
+
 struct WsBars {
   uint64_t* full;        // [2]
   uint64_t* empty;       // [2]
   uint64_t* acc_ready;   // [8]
   uint64_t* acc_free;    // [8]
-  uint64_t* tile_ready;  // [8]
+  int* tile_done;        // [8] completion counters (all matrices of this CTA)
   uint64_t* drain;       // [1]
   uint32_t* tslot;
   volatile int* flag;
@@ -81,22 +119,23 @@ struct WsBars {
 
 // ---------------------------------------------------------------------------
 // Producer: one thread.
-template <int MODE>
-__device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t batch, int n, uint32_t tmem) {
+template <int MODE, int CL>
+__device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t batch, int n, uint32_t tmem,
+                            int rank) {
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
   uint32_t n_load[2] = {0u, 0u}, n_empty[2] = {0u, 0u};
   int writes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t biter = 0;
   bool ok = true;
-  for (int64_t b = blockIdx.x; b < batch && ok; b += gridDim.x, ++biter) {
+  for (int64_t b = blockIdx.x / CL; b < batch && ok; b += gridDim.x / CL, ++biter) {
     const uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     const uint8_t* W1 = W0 + rbytes;
     for (int k = 1; k < N && ok; ++k) {
       const int k0 = k * kWB;
       const int mt_n = (n - k0 + kWM - 1) / kWM;
       const int prev_n = (n - k0 + kWB + kWM - 1) / kWM;
-      const int iters = mt_n * k;
+      const int iters = ws_tile_count<CL>(mt_n, rank) * k;
       // Dependencies of the chunk over column k-1 for tile mt.
       auto deps_ready = [&](int mt, bool block) -> bool {
         int ts[3];
@@ -106,18 +145,15 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
         if (mt + 1 < prev_n) ts[nt++] = mt + 1;
         for (int q = 0; q < nt; ++q) {
           const int t = ts[q];
-          const int64_t idx = biter * (int64_t)(N - 2 * t) + (k - 1);
-          const uint32_t par = (uint32_t)(idx & 1);
-          if (block) {
-            if (!ws_wait(br.tile_ready + t, par, br.flag)) return false;
-          } else if (!umma::mbar_try_wait(br.tile_ready + t, par)) {
-            return false;
-          }
+          // Tile t completes once per block column it exists in (N - 2t per
+          // matrix); column k-1 of this matrix is completion number target.
+          const int target = (int)(biter * (int64_t)(N - 2 * t) + k);
+          if (!ws_wait_count(br.tile_done + t, target, br.flag, block)) return false;
         }
         return true;
       };
       auto issue_load = [&](int i) -> bool {
-        const int mt = i / k, kc = i - (i / k) * k;
+        const int mt = ws_tile_of<CL>(i / k, rank), kc = i - (i / k) * k;
         const int s = i & 1;
         if (n_load[s] > 0) {
           // The stage held the previous chunk: wait until the MMAs that read it completed.
@@ -144,11 +180,11 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
       }
       for (int i = 0; i < iters && ok; ++i) {
         const int s = i & 1;
-        const int mt = i / k, kc = i - (i / k) * k;
+        const int mt = ws_tile_of<CL>(i / k, rank), kc = i - (i / k) * k;
         // Prefetch the next chunk unless it would wait on consumers.
         bool prefetched = false;
         if (next == i + 1 && next < iters) {
-          const int nmt = next / k, nkc = next - (next / k) * k;
+          const int nmt = ws_tile_of<CL>(next / k, rank), nkc = next - (next / k) * k;
           if (nkc != k - 1 || deps_ready(nmt, false)) {
             if (!issue_load(next)) { ok = false; break; }
             ++next;
@@ -187,9 +223,9 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
 
 // ---------------------------------------------------------------------------
 // Consumers: warps 0-7.
-template <int MODE>
+template <int MODE, int CL>
 __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
-                             int n, uint32_t tmem, int32_t* info) {
+                             int n, uint32_t tmem, int32_t* info, int rank) {
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
@@ -198,7 +234,8 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
   uint32_t ready_par = 0u;  // bit t: parity of the next acc_ready phase of tile t
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+  int64_t biter = 0;
+  for (int64_t b = blockIdx.x / CL; b < batch; b += gridDim.x / CL, ++biter) {
     const float* A = a + (size_t)b * n * n;
     float* L = l + (size_t)b * n * n;
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
@@ -208,9 +245,13 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
     for (int k = 0; k < N && !failed; ++k) {
       const int k0 = k * kWB;
       const int mt_n = (n - k0 + kWM - 1) / kWM;
-      for (int mt = 0; mt < mt_n; ++mt) {
+      const int nt = ws_tile_count<CL>(mt_n, rank);
+      for (int j = 0; j < nt; ++j) {
+        const int mt = ws_tile_of<CL>(j, rank);
+        // Rank 1's copy of tile 0: only the diagonal block is used.
+        const bool diag_only = CL == 2 && rank == 1 && mt == 0;
         const int r0 = k0 + mt * kWM;
-        const int vr = min(kWM, n - r0);
+        const int vr = diag_only ? 64 : min(kWM, n - r0);
         // (a) D from TMEM, P = A - D.
         {
           const int w4 = warp & 3, h = warp >> 2;
@@ -251,8 +292,10 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
 #pragma unroll
             for (int q = 0; q < 32; ++q) p[q] = 0.0f;
           }
+          if (!diag_only) {
 #pragma unroll
-          for (int q = 0; q < 32; ++q) PtT[(32 * h + q) * kWPtLd + rl] = p[q];
+            for (int q = 0; q < 32; ++q) PtT[(32 * h + q) * kWPtLd + rl] = p[q];
+          }
           if (mt == 0 && rl < 64) {
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
@@ -267,7 +310,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
           if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
-          for (int e = tid; e < 64 * 16; e += kWConsumers) {
+          for (int e = tid; e < (rank == 0 ? 64 * 16 : 0); e += kWConsumers) {
             const int r = e >> 4, c = (e & 15) * 4;
             const float* srow = dg.S + r * kD64Ld + c;
             const float4 v = make_float4(c <= r ? srow[0] : 0.f, c + 1 <= r ? srow[1] : 0.f,
@@ -277,12 +320,13 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           // Zero strip right of the diagonal block: one bulk store per row from
           // the zero buffer, issued by one thread and left to run.
           const uint32_t strip = 4u * (uint32_t)(n - k0 - kWB);
-          if (tid == 0 && strip > 0) {
+          if (tid == 0 && rank == 0 && strip > 0) {
             for (int r = 0; r < 64; ++r) umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kWB, zeros, strip);
             umma::bulk_commit();
           }
           cbar();
         }
+        if (diag_only) continue;
         // (c) X = P T^T (triangle skipped), then L and the tensor-core copy from X^T.
         xgemm_tri_inplace(PtT, kWPtLd, dg.T, kD64Ld, cbar);
         // Output: first the tensor-core copy, published to the producer's bulk
@@ -297,8 +341,13 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           if (k + 1 < N && rl < vr && !(mt == 0 && rl < 64)) panel_copy_store<MODE>(W0, W1, N, k, r0 + rl, c, v[it]);
         }
         umma::fence_proxy_async_all();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(br.tile_ready + mt);
+        cbar();
+        if (tid == 0) {
+          // Completion number of tile mt: once per block column it exists in.
+          const int done = (int)(biter * (int64_t)(N - 2 * mt) + k + 1);
+          st_release_cluster(br.tile_done + mt, (uint32_t)rank, done);
+          if (CL == 2) st_release_cluster(br.tile_done + mt, (uint32_t)(rank ^ 1), done);
+        }
 #pragma unroll
         for (int it = 0; it < 4; ++it) {
           const int item = tid + kWConsumers * it;
@@ -311,14 +360,14 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
         cbar();
       }
     }
-    if (tid == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
+    if (tid == 0 && rank == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
     if (failed) break;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
 }
 
-template <int MODE>
+template <int MODE, int CL>
 __global__ void __launch_bounds__(kWThreads, 1)
     potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
                           uint8_t* __restrict__ ws, int32_t* __restrict__ info) {
@@ -330,13 +379,14 @@ __global__ void __launch_bounds__(kWThreads, 1)
   br.empty = bars + 2;
   br.acc_ready = bars + 4;
   br.acc_free = bars + 12;
-  br.tile_ready = bars + 20;
+  br.tile_done = reinterpret_cast<int*>(bars + 20);
   br.drain = bars + 28;
   br.tslot = reinterpret_cast<uint32_t*>(bars + 29);
   br.flag = reinterpret_cast<volatile int*>(bars + 30);
   br.badp = reinterpret_cast<int*>(bars + 30) + 1;
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) *br.flag = 0;
+  if (tid < 8) br.tile_done[tid] = 0;
   for (uint32_t e = tid; e < kWZeroBytes / 16; e += kWThreads)
     reinterpret_cast<float4*>(sm + kWZeroOff)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   // The zeros are read by the async proxy (bulk stores).
@@ -349,21 +399,25 @@ __global__ void __launch_bounds__(kWThreads, 1)
     for (int i = 0; i < 4; ++i) umma::mbar_init(bars + i, 1);             // full, empty
     for (int i = 0; i < 8; ++i) umma::mbar_init(br.acc_ready + i, 1);     // tcgen05.commit
     for (int i = 0; i < 8; ++i) umma::mbar_init(br.acc_free + i, 8);      // one arrive per consumer warp
-    for (int i = 0; i < 8; ++i) umma::mbar_init(br.tile_ready + i, 8);
     umma::mbar_init(br.drain, 1);
     umma::mbar_fence_init();
   }
   umma::fence_before_sync();
   __syncthreads();
+  // The peer's barriers are initialised before anyone arrives on them.
+  if (CL == 2) umma::cluster_sync();
   umma::fence_after_sync();
   const uint32_t tmem = *br.tslot;
+  const int rank = CL == 2 ? (int)umma::cluster_rank() : 0;
   if (warp == kWConsumers / 32) {
-    if ((tid & 31) == 0) ws_producer<MODE>(br, sm, ws, batch, n, tmem);
+    if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
-    ws_consumers<MODE>(br, sm, a, l, ws, batch, n, tmem, info);
+    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank);
   }
   umma::fence_before_sync();
   __syncthreads();
+  // No CTA leaves while its peer may still arrive on its barriers.
+  if (CL == 2) umma::cluster_sync();
   if (warp == 0) umma::tmem_dealloc(tmem, kWTmemCols);
 }
 
@@ -373,18 +427,32 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
   uint8_t* wsa = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ws) + 1023) & ~(uintptr_t)1023);
-  const int grid = (int)std::min<int64_t>(batch, (int64_t)device_sms());
+  const int64_t sms = device_sms();
+  // Two CTAs per matrix when the batch leaves at least half the SMs idle.
+  const int cl = (batch * 2 <= sms) ? 2 : 1;
+  const int grid = cl * (int)std::min<int64_t>(batch, sms / cl);
+  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
+  void (*kern)(const float*, float*, int64_t, int, uint8_t*, int32_t*) =
+      tf32 ? (cl == 2 ? potrf_fused_ws_kernel<B2P_MODE_TF32, 2> : potrf_fused_ws_kernel<B2P_MODE_TF32, 1>)
+           : (cl == 2 ? potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2> : potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1>);
+  const int slot = tf32 ? (cl == 2 ? kSlotFusedWs2 : kSlotFusedWs0) : (cl == 2 ? kSlotFusedWs3 : kSlotFusedWs1);
+  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, slot)) return st;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid, 1, 1);
+  cfg.blockDim = dim3(kWThreads, 1, 1);
+  cfg.dynamicSmemBytes = kWSmemBytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   TraceScope ts(kKFusedWs, s);
-  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
-    if (int st = ensure_smem_attr((const void*)potrf_fused_ws_kernel<B2P_MODE_TF32>, kWSmemBytes, kSlotFusedWs0))
-      return st;
-    potrf_fused_ws_kernel<B2P_MODE_TF32><<<grid, kWThreads, kWSmemBytes, s>>>(a, l, batch, n, wsa, info);
-  } else {
-    if (int st = ensure_smem_attr((const void*)potrf_fused_ws_kernel<B2P_MODE_BF16X3>, kWSmemBytes, kSlotFusedWs1))
-      return st;
-    potrf_fused_ws_kernel<B2P_MODE_BF16X3><<<grid, kWThreads, kWSmemBytes, s>>>(a, l, batch, n, wsa, info);
-  }
-  return check_launch("potrf_fused_ws_kernel");
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info);
+  if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
+  return B2P_OK;
 }
 
 }  // namespace b2p

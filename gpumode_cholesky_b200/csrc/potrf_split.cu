@@ -47,25 +47,6 @@ namespace b2p {
 constexpr int kSplitSegCap = 8;  // most K segments per column (= cluster size)
 constexpr uint32_t kSplitPolls = 1u << 24;
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ float4 ld_cluster_f4(const void* local, uint32_t rank) {
-  uint32_t addr;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(umma::smem_u32(local)), "r"(rank));
-  float4 v;
-  asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "r"(addr)
-               : "memory");
-  return v;
-}
-
 // ---- update kernel -----------------------------------------------------------
 constexpr int kUThreads = 128;
 constexpr uint32_t kUStageA = 32768;  // 128 rows x 2 regions
@@ -98,7 +79,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
   const int N = n / 64, k0 = 64 * k;
   const int tiles = (n - k0 + 127) / 128;
   const size_t rbytes = panel_copy_region_bytes(n);
-  const int s = (int)cluster_rank();
+  const int s = (int)umma::cluster_rank();
   const int64_t bt = blockIdx.x / segs;
   const int t = (int)(bt % tiles);
   const int64_t b = bt / tiles;
@@ -200,7 +181,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     info[b] = -1;
   }
   umma::fence_before_sync();
-  cluster_sync_all();
+  umma::cluster_sync();
   // Every CTA of the cluster takes a share of the 128 x 16 float4 of P and
   // sums the parked accumulators of all segments in segment order.
   if (ok) {
@@ -210,7 +191,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
       const int row = e >> 4, c4 = (e & 15) * 4;
       float4 v = *reinterpret_cast<const float4*>(B + (size_t)(r0 + row) * base_ld + c4);
       for (int q = 0; q < segs; ++q) {
-        const float4 u = ld_cluster_f4(park + row * kUParkLd + c4, (uint32_t)q);
+        const float4 u = umma::ld_cluster_f4(park + row * kUParkLd + c4, (uint32_t)q);
         v.x -= u.x;
         v.y -= u.y;
         v.z -= u.z;
@@ -220,7 +201,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     }
   }
   // No CTA leaves while another may still read its parked accumulator.
-  cluster_sync_all();
+  umma::cluster_sync();
   if (!got) umma::mbar_wait_bounded(done, 0u, kSplitPolls);
   umma::fence_after_sync();
   if (warp == 0) umma::tmem_dealloc(tmem, kUTmemCols);

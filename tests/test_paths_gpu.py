@@ -80,6 +80,19 @@ def test_paths_nonspd_info(path, col):
     assert torch.isnan(l[1]).any()
 
 
+@pytest.mark.parametrize("batch,n", [(3, 1024), (40, 576), (150, 256)])
+def test_fused_ws_cluster_and_single(batch, n):
+    """Batches up to half the SM count run two CTAs per matrix; larger ones one."""
+    a = inputs.mixed_batch(batch, n, seed=batch + n, device="cuda")
+    info = torch.full((batch,), -9, dtype=torch.int32, device="cuda")
+    l = cholesky(a, mode="bf16x3", info=info, path="fused_ws")
+    assert (info == 0).all()
+    _check_factor(l, a, "bf16x3")
+    ref = cholesky(a, mode="bf16x3", path="fused").double()
+    d = torch.linalg.norm((l.double() - ref).flatten()) / torch.linalg.norm(ref.flatten())
+    assert d.item() <= TOL_AGREE["bf16x3"]
+
+
 def test_split_repeat_bitwise():
     a = inputs.well_conditioned(2, 1536, seed=4, device="cuda")
     assert torch.equal(cholesky(a, mode="bf16x3", path="split"), cholesky(a, mode="bf16x3", path="split"))
