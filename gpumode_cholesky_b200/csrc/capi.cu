@@ -70,25 +70,25 @@ int ensure_smem_attr(const void* func, size_t bytes, int slot) {
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-static bool path_supported(int path, int64_t n, int mode) {
+static bool path_supported(int path, int64_t batch, int64_t n, int mode) {
   switch (path) {
     case B2P_PATH_BLOCKED: return true;
-    case B2P_PATH_FUSED:
-    case B2P_PATH_FUSED_WS: return fused_supported(n, mode);
+    case B2P_PATH_FUSED: return fused_supported(n, mode);
+    case B2P_PATH_FUSED_WS: return fused_ws_supported(batch, n, mode);
     case B2P_PATH_SPLIT: return split_supported(n, mode);
     default: return false;
   }
 }
 
-// The n > 128 algorithm for (batch, n, mode).  Measured on B200 (BF16x3):
-// one CTA per matrix wins while the batch gives each SM most of a matrix
-// (60x1024: 932 us vs 1065 split; 16x512: 246 vs 254); a handful of large
-// matrices is faster spread over the GPU (4x1024: 511 vs 903).
+// The n > 128 algorithm for (batch, n, mode).  Tensor modes, measured on
+// B200 (BF16x3): up to n = 1024 one CTA per matrix while the batch fills
+// the GPU (640x512: 1225 us), else the warp-specialized kernel in clusters of
+// up to 8 CTAs per matrix (60x1024: 646 us, 4x1024: 421 us); above 1024 the
+// multi-CTA split path (8x2048: 1351 us).  FP32: blocked.
 static int choose_path(int64_t batch, int64_t n, int mode) {
   const int64_t sms = device_sms();
-  if (split_supported(n, mode) && (!fused_supported(n, mode) || (n >= 512 && batch * 16 <= sms)))
-    return B2P_PATH_SPLIT;
   if (fused_supported(n, mode)) return batch > sms ? B2P_PATH_FUSED : B2P_PATH_FUSED_WS;
+  if (split_supported(n, mode)) return B2P_PATH_SPLIT;
   return B2P_PATH_BLOCKED;
 }
 
@@ -137,7 +137,7 @@ size_t b2p_potrf_workspace_size(int64_t batch, int64_t n, int mode) {
 size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int path) {
   if (batch <= 0 || n <= 128 || check_mode(mode) != B2P_OK) return 0;
   if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
-  if (!path_supported(path, n, mode)) return 0;
+  if (!path_supported(path, batch, n, mode)) return 0;
   return path_workspace_bytes(path, batch, n, mode);
 }
 
@@ -164,7 +164,7 @@ int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, i
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
   if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
-  if (!path_supported(path, n, mode))
+  if (!path_supported(path, batch, n, mode))
     return set_error(B2P_ERR_UNSUPPORTED, "path %d does not support n=%lld mode 0x%x", path, (long long)n, mode);
   switch (path) {
     case B2P_PATH_FUSED: return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);

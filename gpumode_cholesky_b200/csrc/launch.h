@@ -42,9 +42,13 @@ bool fused_supported(int64_t n, int mode);
 size_t fused_workspace_bytes(int64_t batch, int64_t n);
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s);
-// Warp-specialized variant (potrf_fused_ws.cu): same workspace and contract.
+// Warp-specialized variant (potrf_fused_ws.cu), in clusters of up to 8 CTAs
+// per matrix for small batches: same workspace and contract.
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                    int32_t* info, cudaStream_t s);
+// Orders and batches the warp-specialized kernel can take (n <= 8192; for
+// n > 1024 the batch must leave room for clusters large enough for TMEM).
+bool fused_ws_supported(int64_t batch, int64_t n, int mode);
 
 // Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
 // n > 128, tensor modes; two launches per 64-wide block column.
@@ -132,6 +136,10 @@ enum SmemSlot {
   kSlotFusedWs1,
   kSlotFusedWs2,
   kSlotFusedWs3,
+  kSlotFusedWs4,
+  kSlotFusedWs5,
+  kSlotFusedWs6,
+  kSlotFusedWs7,
   kSlotSplitU0,
   kSlotSplitU1,
   kSlotSplitS0,

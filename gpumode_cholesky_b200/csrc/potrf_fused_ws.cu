@@ -13,10 +13,10 @@
 //        block (tile 0), X = P T^T in FP32, write L and the tensor-core copy
 //        of X, then publish the tile's completion count.
 //
-// Small batches run as clusters of two CTAs per matrix (CL = 2): rank 0 takes
-// the even row tiles of every block column (tile 0 holds the diagonal block),
-// rank 1 the odd ones, and rank 1 also accumulates its own copy of tile 0 to
-// factor the diagonal block redundantly, so the two CTAs share only panel
+// Small batches run as clusters of CL = 2, 4 or 8 CTAs per matrix: rank r
+// takes the row tiles t = r (mod CL) of every block column (tile 0 holds the
+// diagonal block), and every rank > 0 also accumulates its own copy of tile
+// 0 to factor the diagonal block redundantly, so the CTAs share only panel
 // copies in global memory.  A finished tile is announced to both CTAs'
 // producers through per-tile completion counters (release stores at cluster
 // scope, bounded acquire polls), which cannot alias the way an mbarrier
@@ -57,9 +57,12 @@ constexpr uint32_t kWStage = kWStageA + 16384;
 constexpr uint32_t kWDiagOff = 2 * kWStage;
 constexpr uint32_t kWPtOff = kWDiagOff + (((uint32_t)sizeof(Diag64Smem) + 1023u) & ~1023u);
 constexpr uint32_t kWZeroOff = kWPtOff + 64 * kWPtLd * 4;  // zeros, source of the strip's bulk stores
-constexpr uint32_t kWZeroBytes = 4096;                    // >= 4 (n - 64) bytes for n <= 1024
+constexpr uint32_t kWZeroBytes = 4096;                    // strip rows are stored in chunks of this
 constexpr uint32_t kWBarOff = kWZeroOff + kWZeroBytes;
-constexpr uint32_t kWSmemBytes = kWBarOff + 256 + 1024;
+constexpr uint32_t kWCntOff = kWBarOff + 256;  // per-tile completion counters
+constexpr int kWMaxTiles = 64;                  // row tiles of a block column (n <= 8192)
+constexpr int kWMaxSlots = 8;                   // TMEM accumulator slots (512 columns)
+constexpr uint32_t kWSmemBytes = kWCntOff + 4 * kWMaxTiles + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
 
@@ -95,14 +98,20 @@ __device__ __forceinline__ bool ws_wait_count(const int* p, int target, volatile
 }
 
 // Row tiles of a block column (mt_n of them) that CTA `rank` of a CL-CTA
-// cluster accumulates: j-th tile and count.
+// cluster accumulates, as a list: rank 0 takes tiles 0, CL, 2 CL, ...; rank
+// r > 0 takes its own copy of tile 0 (for the diagonal block) and tiles r,
+// r + CL, ...  Entry j of the list uses TMEM slot j.
 template <int CL>
 __device__ __forceinline__ int ws_tile_count(int mt_n, int rank) {
-  return CL == 1 ? mt_n : (rank == 0 ? (mt_n + 1) / 2 : 1 + mt_n / 2);
+  if (CL == 1) return mt_n;
+  if (rank == 0) return (mt_n + CL - 1) / CL;
+  return 1 + (mt_n > rank ? (mt_n - rank + CL - 1) / CL : 0);
 }
 template <int CL>
 __device__ __forceinline__ int ws_tile_of(int j, int rank) {
-  return CL == 1 ? j : (rank == 0 ? 2 * j : (j == 0 ? 0 : 2 * j - 1));
+  if (CL == 1) return j;
+  if (rank == 0) return j * CL;
+  return j == 0 ? 0 : rank + (j - 1) * CL;
 }
 
 struct WsBars {
@@ -110,7 +119,7 @@ struct WsBars {
   uint64_t* empty;       // [2]
   uint64_t* acc_ready;   // [8]
   uint64_t* acc_free;    // [8]
-  int* tile_done;        // [8] completion counters (all matrices of this CTA)
+  int* tile_done;        // [kWMaxTiles] completion counters (all matrices of this CTA)
   uint64_t* drain;       // [1]
   uint32_t* tslot;
   volatile int* flag;
@@ -125,7 +134,7 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
   uint32_t n_load[2] = {0u, 0u}, n_empty[2] = {0u, 0u};
-  int writes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int writes[kWMaxSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t biter = 0;
   bool ok = true;
   for (int64_t b = blockIdx.x / CL; b < batch && ok; b += gridDim.x / CL, ++biter) {
@@ -180,7 +189,7 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
       }
       for (int i = 0; i < iters && ok; ++i) {
         const int s = i & 1;
-        const int mt = ws_tile_of<CL>(i / k, rank), kc = i - (i / k) * k;
+        const int slot = i / k, kc = i - (i / k) * k;
         // Prefetch the next chunk unless it would wait on consumers.
         bool prefetched = false;
         if (next == i + 1 && next < iters) {
@@ -192,18 +201,18 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
           }
         }
         if (!ws_wait(br.full + s, (n_load[s] - 1u) & 1u, br.flag)) { ok = false; break; }
-        if (kc == 0 && writes[mt] > 0) {
-          // TMEM tile mt must have been read by the consumers.
-          if (!ws_wait(br.acc_free + mt, (uint32_t)((writes[mt] - 1) & 1), br.flag)) { ok = false; break; }
+        if (kc == 0 && writes[slot] > 0) {
+          // TMEM slot `slot` must have been read by the consumers.
+          if (!ws_wait(br.acc_free + slot, (uint32_t)((writes[slot] - 1) & 1), br.flag)) { ok = false; break; }
         }
         umma::fence_after_sync();
         const uint32_t st = umma::smem_u32(sm + s * kWStage);
-        panel_copy_mmas<MODE>(tmem + (uint32_t)(kWB * mt), st, st + kWStageA, kc > 0);
+        panel_copy_mmas<MODE>(tmem + (uint32_t)(kWB * slot), st, st + kWStageA, kc > 0);
         umma::mma_commit(br.empty + s);
         ++n_empty[s];
         if (kc == k - 1) {
-          umma::mma_commit(br.acc_ready + mt);
-          ++writes[mt];
+          umma::mma_commit(br.acc_ready + slot);
+          ++writes[slot];
         }
         if (!prefetched && next == i + 1 && next < iters) {
           if (!issue_load(next)) { ok = false; break; }
@@ -248,8 +257,8 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
       const int nt = ws_tile_count<CL>(mt_n, rank);
       for (int j = 0; j < nt; ++j) {
         const int mt = ws_tile_of<CL>(j, rank);
-        // Rank 1's copy of tile 0: only the diagonal block is used.
-        const bool diag_only = CL == 2 && rank == 1 && mt == 0;
+        // A copy of tile 0 on rank > 0: only the diagonal block is used.
+        const bool diag_only = CL > 1 && rank != 0 && mt == 0;
         const int r0 = k0 + mt * kWM;
         const int vr = diag_only ? 64 : min(kWM, n - r0);
         // (a) D from TMEM, P = A - D.
@@ -258,8 +267,8 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           const int rl = 32 * w4 + lane;
           float d[32];
           if (k > 0) {
-            const bool got = ws_wait(br.acc_ready + mt, (ready_par >> mt) & 1u, br.flag);
-            ready_par ^= 1u << mt;
+            const bool got = ws_wait(br.acc_ready + j, (ready_par >> j) & 1u, br.flag);
+            ready_par ^= 1u << j;
             if (!got) *br.flag = 1;
           }
           cbar();
@@ -269,10 +278,10 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           }
           if (k > 0) {
             umma::fence_after_sync();
-            umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kWB * mt + 32 * h), d);
+            umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kWB * j + 32 * h), d);
             umma::fence_before_sync();
             __syncwarp();
-            if (lane == 0) mbar_arrive(br.acc_free + mt);
+            if (lane == 0) mbar_arrive(br.acc_free + j);
           } else {
 #pragma unroll
             for (int q = 0; q < 32; ++q) d[q] = 0.0f;
@@ -321,7 +330,11 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           // the zero buffer, issued by one thread and left to run.
           const uint32_t strip = 4u * (uint32_t)(n - k0 - kWB);
           if (tid == 0 && rank == 0 && strip > 0) {
-            for (int r = 0; r < 64; ++r) umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kWB, zeros, strip);
+            for (int r = 0; r < 64; ++r) {
+              uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + kWB);
+              for (uint32_t off = 0; off < strip; off += kWZeroBytes)
+                umma::bulk_s2g(row + off, zeros, min(kWZeroBytes, strip - off));
+            }
             umma::bulk_commit();
           }
           cbar();
@@ -345,8 +358,8 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
         if (tid == 0) {
           // Completion number of tile mt: once per block column it exists in.
           const int done = (int)(biter * (int64_t)(N - 2 * mt) + k + 1);
-          st_release_cluster(br.tile_done + mt, (uint32_t)rank, done);
-          if (CL == 2) st_release_cluster(br.tile_done + mt, (uint32_t)(rank ^ 1), done);
+#pragma unroll
+          for (int q = 0; q < CL; ++q) st_release_cluster(br.tile_done + mt, (uint32_t)q, done);
         }
 #pragma unroll
         for (int it = 0; it < 4; ++it) {
@@ -379,14 +392,14 @@ __global__ void __launch_bounds__(kWThreads, 1)
   br.empty = bars + 2;
   br.acc_ready = bars + 4;
   br.acc_free = bars + 12;
-  br.tile_done = reinterpret_cast<int*>(bars + 20);
+  br.tile_done = reinterpret_cast<int*>(sm + kWCntOff);
   br.drain = bars + 28;
   br.tslot = reinterpret_cast<uint32_t*>(bars + 29);
   br.flag = reinterpret_cast<volatile int*>(bars + 30);
   br.badp = reinterpret_cast<int*>(bars + 30) + 1;
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) *br.flag = 0;
-  if (tid < 8) br.tile_done[tid] = 0;
+  if (tid < kWMaxTiles) br.tile_done[tid] = 0;
   for (uint32_t e = tid; e < kWZeroBytes / 16; e += kWThreads)
     reinterpret_cast<float4*>(sm + kWZeroOff)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
   // The zeros are read by the async proxy (bulk stores).
@@ -405,10 +418,10 @@ __global__ void __launch_bounds__(kWThreads, 1)
   umma::fence_before_sync();
   __syncthreads();
   // The peer's barriers are initialised before anyone arrives on them.
-  if (CL == 2) umma::cluster_sync();
+  if (CL > 1) umma::cluster_sync();
   umma::fence_after_sync();
   const uint32_t tmem = *br.tslot;
-  const int rank = CL == 2 ? (int)umma::cluster_rank() : 0;
+  const int rank = CL > 1 ? (int)umma::cluster_rank() : 0;
   if (warp == kWConsumers / 32) {
     if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
@@ -417,8 +430,33 @@ __global__ void __launch_bounds__(kWThreads, 1)
   umma::fence_before_sync();
   __syncthreads();
   // No CTA leaves while its peer may still arrive on its barriers.
-  if (CL == 2) umma::cluster_sync();
+  if (CL > 1) umma::cluster_sync();
   if (warp == 0) umma::tmem_dealloc(tmem, kWTmemCols);
+}
+
+// CTAs per matrix for (batch, n): as many as the SMs allow (up to the
+// portable cluster size of 8, no more than a block column has row tiles),
+// and at least enough that every rank's tile list fits the TMEM slots.
+// 0 if n needs more than 8.
+static int ws_cluster_size(int64_t batch, int n) {
+  const int mt_n = (n + kWM - 1) / kWM;
+  int need = 1;
+  while (need <= 8 && (mt_n + need - 1) / need + (need > 1 ? 1 : 0) > kWMaxSlots) need *= 2;
+  if (need > 8 || mt_n > kWMaxTiles) return 0;
+  const int64_t sms = device_sms();
+  int cl = need;
+  while (cl < 8 && batch * cl * 2 <= sms && cl * 2 <= mt_n) cl *= 2;
+  return cl;
+}
+
+// Orders up to 1024.  Larger ones would fit (clusters big enough for TMEM),
+// but with K up to n every CTA then streams its whole row range of panel
+// copies per block column and is bound by its own bulk-copy bandwidth
+// (8x2048: 1630 us against 1351 us on the split path; 1x4096: 7490 vs 2335).
+bool fused_ws_supported(int64_t batch, int64_t n, int mode) {
+  const int m = mode & B2P_MODE_MASK;
+  return (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3) && !(mode & B2P_FLAG_FP64_DIAG) && n > 128 && n % 64 == 0 &&
+         n <= 1024 && ws_cluster_size(batch, (int)n) > 0;
 }
 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
@@ -428,15 +466,20 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
   uint8_t* wsa = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ws) + 1023) & ~(uintptr_t)1023);
   const int64_t sms = device_sms();
-  // Two CTAs per matrix when the batch leaves at least half the SMs idle.
-  const int cl = (batch * 2 <= sms) ? 2 : 1;
-  const int grid = cl * (int)std::min<int64_t>(batch, sms / cl);
+  const int cl = ws_cluster_size(batch, n);
+  if (cl == 0 || !fused_ws_supported(batch, n, mode))
+    return set_error(B2P_ERR_UNSUPPORTED, "warp-specialized path: n=%d not supported", n);
+  const int grid = cl * (int)std::max<int64_t>(1, std::min<int64_t>(batch, sms / cl));
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  void (*kern)(const float*, float*, int64_t, int, uint8_t*, int32_t*) =
-      tf32 ? (cl == 2 ? potrf_fused_ws_kernel<B2P_MODE_TF32, 2> : potrf_fused_ws_kernel<B2P_MODE_TF32, 1>)
-           : (cl == 2 ? potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2> : potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1>);
-  const int slot = tf32 ? (cl == 2 ? kSlotFusedWs2 : kSlotFusedWs0) : (cl == 2 ? kSlotFusedWs3 : kSlotFusedWs1);
-  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, slot)) return st;
+  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*);
+  static const Kern kernels[2][4] = {
+      {potrf_fused_ws_kernel<B2P_MODE_TF32, 1>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2>,
+       potrf_fused_ws_kernel<B2P_MODE_TF32, 4>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8>},
+      {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2>,
+       potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8>}};
+  const int li = cl == 1 ? 0 : cl == 2 ? 1 : cl == 4 ? 2 : 3;
+  const Kern kern = kernels[tf32 ? 0 : 1][li];
+  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, kSlotFusedWs0 + (tf32 ? 0 : 4) + li)) return st;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid, 1, 1);
   cfg.blockDim = dim3(kWThreads, 1, 1);

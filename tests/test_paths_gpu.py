@@ -80,14 +80,15 @@ def test_paths_nonspd_info(path, col):
     assert torch.isnan(l[1]).any()
 
 
-@pytest.mark.parametrize("batch,n", [(3, 1024), (40, 576), (150, 256)])
+@pytest.mark.parametrize("batch,n", [(3, 1024), (5, 768), (16, 512), (40, 576), (150, 256)])
 def test_fused_ws_cluster_and_single(batch, n):
-    """Batches up to half the SM count run two CTAs per matrix; larger ones one."""
+    """Small batches run 8, 4 or 2 CTAs per matrix; batches above half the SM count one."""
     a = inputs.mixed_batch(batch, n, seed=batch + n, device="cuda")
     info = torch.full((batch,), -9, dtype=torch.int32, device="cuda")
     l = cholesky(a, mode="bf16x3", info=info, path="fused_ws")
     assert (info == 0).all()
     _check_factor(l, a, "bf16x3")
+    # Same arithmetic as the one-CTA-per-matrix kernel.
     ref = cholesky(a, mode="bf16x3", path="fused").double()
     d = torch.linalg.norm((l.double() - ref).flatten()) / torch.linalg.norm(ref.flatten())
     assert d.item() <= TOL_AGREE["bf16x3"]
@@ -109,5 +110,7 @@ def test_unsupported_path_raises():
     a = inputs.well_conditioned(1, 2048, seed=1, device="cuda")
     with pytest.raises(Exception, match="unsupported"):
         cholesky(a, mode="bf16x3", path="fused")
+    with pytest.raises(Exception, match="unsupported"):
+        cholesky(a, mode="bf16x3", path="fused_ws")
     with pytest.raises(Exception, match="unsupported"):
         cholesky(a, mode="fp32", path="split")
