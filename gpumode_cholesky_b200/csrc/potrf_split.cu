@@ -15,16 +15,17 @@
 //       after a cluster barrier the CTAs together form
 //           P = base[r0:r0+128] - U_0 - U_1 - ...
 //       (fixed order, read over distributed shared memory) into a per-matrix
-//       FP32 panel buffer; base is A's block column or, for the second of a
-//       column's two update launches, the panel buffer itself (see the
-//       schedule above potrf_split).
-//   split_step_kernel(k)    G CTAs per matrix.  Every CTA factors the
-//       diagonal block P[k0:k0+64] in shared memory (diag64_factor) --
+//       FP32 panel buffer, over all but the newest earlier panel ("look-ahead",
+//       see the schedule above potrf_split).
+//   split_step_kernel(k)    G CTAs per matrix.  Every CTA applies the newest
+//       panel k-1 to the diagonal rows and to its own 128-row chunk on
+//       tcgen05 (bulk copies of the panel copy, one TMEM lane per row),
+//       factors the diagonal block in shared memory (diag64_factor) --
 //       redundantly, which costs one diagonal engine per CTA but no extra
-//       launch or grid-wide wait -- then solves its rows of the panel by
-//       forward substitution, one row per thread (X L_kk^T = P, FP32), and
-//       writes L and the panel copy of X.  CTA 0 of the matrix writes L_kk and
-//       info; the zero strip right of the diagonal block is shared out.
+//       launch or grid-wide wait -- then solves its rows by forward
+//       substitution, one row per thread (X L_kk^T = P, FP32), and writes L
+//       and the panel copy of X.  CTA 0 of the matrix writes L_kk and info;
+//       the zero strip right of the diagonal block goes out as bulk stores.
 //
 // A is read once and L written once; the panel copies (4 bytes per element
 // in either mode) are the only re-read data and mostly hit L2.  Results are
@@ -209,40 +210,136 @@ __global__ void __launch_bounds__(kUThreads, 2)
 
 // ---- step kernel -------------------------------------------------------------
 constexpr int kSThreads = 128;
-constexpr uint32_t kSSmemBytes = (uint32_t)sizeof(Diag64Smem) + 128;
+constexpr uint32_t kSB = 0;            // panel k-1 rows k0..k0+63 (B operand): 2 x 8 KB
+constexpr uint32_t kSAd = 16384;       // the same rows as an A operand (64 of 128 rows)
+constexpr uint32_t kSAo = 49152;       // the CTA's 128 rows of panel k-1
+constexpr uint32_t kSZero = 81920;     // zeros for the strip's bulk stores
+constexpr uint32_t kSZeroBytes = 4096;
+constexpr uint32_t kSDiag = kSZero + kSZeroBytes;
+constexpr uint32_t kSBar = kSDiag + (((uint32_t)sizeof(Diag64Smem) + 127u) & ~127u);
+constexpr uint32_t kSSmemBytes = kSBar + 64 + 1024;
+constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the CTA's rows
 
-// Rows of the panel below the diagonal block are handled in chunks of
-// kSThreads rows, chunk q = rows k0 + 64 + 128 q ..; CTA g of the matrix
-// takes chunks g, g + G, ...  P comes from A (k == 0) or the panel buffer.
+// Column k of every matrix, G CTAs per matrix.  P = base - X_{k-1} X_{k-1,kk}^T
+// where base is A (k <= 1) or the panel buffer holding A minus the panels
+// 0..k-2 (look-ahead), and the newest panel k-1 is applied here on tcgen05
+// from its panel copy.  Then: factor the diagonal block (every CTA), solve
+// the CTA's 128-row chunks by forward substitution (one row per thread,
+// which is also one TMEM lane per thread), write L and the panel copy.
 template <int MODE>
-__global__ void __launch_bounds__(kSThreads, 4)
+__global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
                       int32_t* __restrict__ info) {
   extern __shared__ unsigned char sraw[];
-  Diag64Smem& dg =
-      *reinterpret_cast<Diag64Smem*>((reinterpret_cast<uintptr_t>(sraw) + 127) & ~(uintptr_t)127);
-  const int tid = threadIdx.x;
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
+  Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kSBar);
+  uint64_t* done = full + 1;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSBar + 16);
+  int* flag = reinterpret_cast<int*>(sm + kSBar + 24);
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int N = n / 64, k0 = 64 * k;
   const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
   const size_t rbytes = panel_copy_region_bytes(n);
   const size_t n2 = (size_t)n * n;
+  const bool upd = k >= 1;
 
-  for (int64_t job = blockIdx.x; job < batch * G; job += gridDim.x) {
+  for (uint32_t e = tid; e < kSZeroBytes / 16; e += kSThreads)
+    reinterpret_cast<float4*>(sm + kSZero)[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  umma::fence_proxy_async_smem();
+  if (tid == 0) *flag = 0;
+  if (upd && warp == 0) {
+    umma::tmem_alloc(tslot, kSTmemCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 32) {
+    umma::mbar_init(full, 1);
+    umma::mbar_init(done, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = upd ? *tslot : 0u;
+  uint32_t ph_full = 0u, ph_done = 0u;
+  bool ok = true;
+
+  for (int64_t job = blockIdx.x; job < batch * G && ok; job += gridDim.x) {
     const int64_t b = job / G;
     const int g = (int)(job - b * G);
     float* L = l + (size_t)b * n2;
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     uint8_t* W1 = W0 + rbytes;
-    // Row r, column k0 + c of P is psrc[r * pld + c].
-    const float* psrc = (k == 0) ? a + (size_t)b * n2 + k0 : pbuf + (size_t)b * n * 64;  // pbuf: this column's buffer
-    const size_t pld = (k == 0) ? (size_t)n : 64;
+    const float* base = (k >= 2) ? pbuf + (size_t)b * n * 64 : a + (size_t)b * n2 + k0;
+    const size_t bld = (k >= 2) ? 64 : (size_t)n;
 
-    for (int e = tid; e < 64 * 16; e += kSThreads) {
-      const int r = e >> 4, c = (e & 15) * 4;
-      *reinterpret_cast<float4*>(dg.S + r * kD64Ld + c) =
-          *reinterpret_cast<const float4*>(psrc + (size_t)(k0 + r) * pld + c);
+    // The newest panel's product for the diagonal rows and chunk q (or the
+    // diagonal rows only when q is out of range); false on a timeout.
+    auto newest_panel = [&](int q, bool first) -> bool {
+      const bool own = q < chunks;
+      const int r0 = k0 + 64 + q * kSThreads;
+      const uint32_t vr = own ? (uint32_t)min(kSThreads, n - r0) : 0u;
+      if (tid == 0) {
+        const size_t boff = panel_copy_row_byte(N, k - 1, k0);
+        umma::mbar_arrive_expect_tx(full, (first ? 4u * 8192u : 0u) + 2u * vr * 128u);
+        if (first) {
+          umma::bulk_g2s(sm + kSB, W0 + boff, 8192u, full);
+          umma::bulk_g2s(sm + kSB + 8192, W1 + boff, 8192u, full);
+          umma::bulk_g2s(sm + kSAd, W0 + boff, 8192u, full);
+          umma::bulk_g2s(sm + kSAd + 16384, W1 + boff, 8192u, full);
+        }
+        if (own) {
+          const size_t aoff = panel_copy_row_byte(N, k - 1, r0);
+          umma::bulk_g2s(sm + kSAo, W0 + aoff, vr * 128u, full);
+          umma::bulk_g2s(sm + kSAo + 16384, W1 + aoff, vr * 128u, full);
+        }
+        if (umma::mbar_wait_bounded(full, ph_full, kSplitPolls)) {
+          umma::fence_after_sync();
+          const uint32_t sb = umma::smem_u32(sm + kSB);
+          if (first) panel_copy_mmas<MODE>(tmem, umma::smem_u32(sm + kSAd), sb, false);
+          if (own) panel_copy_mmas<MODE>(tmem + 64, umma::smem_u32(sm + kSAo), sb, false);
+        } else {
+          *flag = 1;
+        }
+        umma::mma_commit(done);
+      }
+      ph_full ^= 1u;
+      const bool got = umma::mbar_wait_bounded(done, ph_done, kSplitPolls);
+      ph_done ^= 1u;
+      umma::fence_after_sync();
+      if (!got) *flag = 1;
+      __syncthreads();
+      return *flag == 0;
+    };
+
+    // 1. Diagonal block: P_kk = base - D (rows k0..k0+63), into dg.S.
+    if (upd && !newest_panel(g, true)) {
+      ok = false;
+      if (tid == 0 && info != nullptr) info[b] = -1;
+      break;
     }
+    if (warp < 2) {
+      const float4* src = reinterpret_cast<const float4*>(base + (size_t)(k0 + tid) * bld);
+      float4* dst = reinterpret_cast<float4*>(dg.S + tid * kD64Ld);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float d[32];
+        if (upd) {
+          umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * h), d);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) d[c] = 0.0f;
+        }
+#pragma unroll
+        for (int c4 = 0; c4 < 8; ++c4) {
+          const float4 v = src[8 * h + c4];
+          dst[8 * h + c4] =
+              make_float4(v.x - d[4 * c4], v.y - d[4 * c4 + 1], v.z - d[4 * c4 + 2], v.w - d[4 * c4 + 3]);
+        }
+      }
+    }
+    umma::fence_before_sync();
     __syncthreads();
     const int bad = diag64_factor(dg);
     if (g == 0) {
@@ -262,28 +359,50 @@ __global__ void __launch_bounds__(kSThreads, 4)
           info[b] = k0 + bad + 1;
       }
     }
-    // Zero strip right of the diagonal block, shared by the matrix's CTAs.
-    {
-      const int s4 = (n - k0 - 64) >> 2;
-      const int64_t total = (int64_t)64 * s4;
-      for (int64_t e = (int64_t)g * kSThreads + tid; e < total; e += (int64_t)G * kSThreads) {
-        const int r = (int)(e / s4), q = (int)(e - (int64_t)r * s4);
-        reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + 64)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    // 2. Zero strip right of the diagonal block: rows g, g + G, ... of it as
+    //    bulk stores from the zero buffer.
+    if (tid == 0) {
+      const uint32_t strip = 4u * (uint32_t)(n - k0 - 64);
+      if (strip > 0) {
+        for (int r = g; r < 64; r += G) {
+          uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + 64);
+          for (uint32_t off = 0; off < strip; off += kSZeroBytes)
+            umma::bulk_s2g(row + off, sm + kSZero, min(kSZeroBytes, strip - off));
+        }
+        umma::bulk_commit();
       }
     }
-    // Panel rows: X L_kk^T = P, one row per thread.
+    // 3. Panel rows: X L_kk^T = P, one row (and one TMEM lane) per thread.
     for (int q = g; q < chunks; q += G) {
+      if (upd && q != g && !newest_panel(q, false)) {
+        ok = false;
+        if (tid == 0 && info != nullptr) info[b] = -1;
+        break;
+      }
       const int r = k0 + 64 + q * kSThreads + tid;
+      float d0[32], d1[32];
+      if (upd) {
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 64u, d0);
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 96u, d1);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) d0[c] = d1[c] = 0.0f;
+      }
       if (r < n) {
         float x[64];
-        const float4* src = reinterpret_cast<const float4*>(psrc + (size_t)r * pld);
+        const float4* src = reinterpret_cast<const float4*>(base + (size_t)r * bld);
 #pragma unroll
-        for (int c4 = 0; c4 < 16; ++c4) {
+        for (int c4 = 0; c4 < 8; ++c4) {
           const float4 v = src[c4];
-          x[4 * c4 + 0] = v.x;
-          x[4 * c4 + 1] = v.y;
-          x[4 * c4 + 2] = v.z;
-          x[4 * c4 + 3] = v.w;
+          x[4 * c4 + 0] = v.x - d0[4 * c4 + 0];
+          x[4 * c4 + 1] = v.y - d0[4 * c4 + 1];
+          x[4 * c4 + 2] = v.z - d0[4 * c4 + 2];
+          x[4 * c4 + 3] = v.w - d0[4 * c4 + 3];
+          const float4 w = src[8 + c4];
+          x[32 + 4 * c4 + 0] = w.x - d1[4 * c4 + 0];
+          x[32 + 4 * c4 + 1] = w.y - d1[4 * c4 + 1];
+          x[32 + 4 * c4 + 2] = w.z - d1[4 * c4 + 2];
+          x[32 + 4 * c4 + 3] = w.w - d1[4 * c4 + 3];
         }
         panel_solve64(x, dg);
         float4* dst = reinterpret_cast<float4*>(L + (size_t)r * n + k0);
@@ -298,10 +417,19 @@ __global__ void __launch_bounds__(kSThreads, 4)
           }
         }
       }
+      // TMEM and the A staging are rewritten by the next chunk.
+      umma::fence_before_sync();
+      __syncthreads();
     }
     // dg is rewritten by the next job.
     __syncthreads();
   }
+  if (!ok) umma::mbar_wait_bounded(done, ph_done, kSplitPolls);
+  // The strip's bulk stores read the zero buffer until they complete.
+  if (tid == 0) umma::bulk_wait_all();
+  umma::fence_before_sync();
+  __syncthreads();
+  if (upd && warp == 0) umma::tmem_dealloc(tmem, kSTmemCols);
 }
 
 // ---- host side -----------------------------------------------------------------
@@ -350,12 +478,11 @@ int side_stream(SideStream** out) {
 
 // Schedule.  Block column j needs every earlier panel.  Panels 0..j-2 are
 // final one step early, so their part of the update ("look-ahead", into the
-// panel buffer of j) runs on the side stream while step j-1 runs; on the
-// caller's stream only the newest panel j-1 ("tail") sits between step j-1
-// and step j:
-//   caller: tail(j) -> step(j) -> [fork] -> tail(j+1) -> step(j+1) -> ...
-//   side:                          look-ahead(j+2) over panels 0..j
-// tail(j) waits for look-ahead(j) (join event j % 2).  Column j uses panel
+// panel buffer of j) runs on the side stream beside step j-1; step j itself
+// applies the newest panel j-1:
+//   caller: step(j) -> [fork] -> step(j+1) -> ...
+//   side:                look-ahead(j+2) over panels 0..j
+// step(j) waits for look-ahead(j) (join event j % 2).  Column j uses panel
 // buffer j % 2, which look-ahead(j+2) may only overwrite after step(j).
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s) {
@@ -403,6 +530,12 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_update_kernel: %s", cudaGetErrorString(e));
     return B2P_OK;
   };
+  // Step CTAs of column k (one per SM).
+  auto step_ctas = [&](int k) -> int64_t {
+    const int chunks = (n - 64 * k - 64 + kSThreads - 1) / kSThreads;
+    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), sms / batch));
+    return std::min<int64_t>(batch * G, sms);
+  };
   auto check = [](cudaError_t e, const char* what) -> int {
     return e == cudaSuccess ? B2P_OK : set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   };
@@ -410,27 +543,22 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   for (int k = 0; k < N; ++k) {
     const int k0 = 64 * k;
     float* pk = pb[k & 1];
-    if (k >= 1) {
-      // Tail: panel k-1, onto the look-ahead result (k >= 2) or onto A.
-      if (k >= 2) {
-        if (int st = check(cudaStreamWaitEvent(s, side->join[k & 1], 0), "cudaStreamWaitEvent")) return st;
-        if (int st = launch_update(k, k - 1, k, pk, (int64_t)n * 64, 64, pk, s, 2)) return st;
-      } else {
-        if (int st = launch_update(k, k - 1, k, a + k0, n2, n, pk, s, 2)) return st;
-      }
+    // Column k >= 2 reads the look-ahead result (panels 0..k-2) from pk.
+    if (k >= 2) {
+      if (int st = check(cudaStreamWaitEvent(s, side->join[k & 1], 0), "cudaStreamWaitEvent")) return st;
     }
-    // Step: CTAs per matrix for about four CTAs per SM in total.
+    // Step (with the newest panel k-1): one CTA per SM in total.
     const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
-    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), 4 * sms / batch));
-    const int grid = (int)std::min<int64_t>(batch * G, 4 * sms);
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), sms / batch));
+    const int grid = (int)step_ctas(k);
     {
       TraceScope ts(kKSplitStep, s);
       stp<<<grid, kSThreads, kSSmemBytes, s>>>(a, l, copies, pk, batch, n, k, G, info);
       if (int st = check_launch("split_step_kernel")) return st;
     }
-    // Look-ahead for column k + 2 over panels 0..k (all final now), at about
-    // one CTA per SM so that the caller's stream keeps room for its tail and
-    // step launches.
+    // Look-ahead for column k + 2 over panels 0..k (all final now), beside
+    // step k + 1.  About one CTA per SM: two of its CTAs fit on an SM, so the
+    // scheduler leaves SMs free for the step.
     if (k + 2 < N) {
       if (int st = check(cudaEventRecord(side->fork, s), "cudaEventRecord")) return st;
       if (int st = check(cudaStreamWaitEvent(side->stream, side->fork, 0), "cudaStreamWaitEvent")) return st;
