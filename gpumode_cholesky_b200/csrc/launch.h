@@ -144,6 +144,7 @@ enum SmemSlot {
   kSlotSplitU1,
   kSlotSplitS0,
   kSlotSplitS1,
+  kSlotBwdSmall,
   kSlotCount
 };
 

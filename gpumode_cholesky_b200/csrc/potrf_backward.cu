@@ -8,9 +8,11 @@
 //   S  = U^T Z                       ( = L^{-T} P L^{-1} )
 //   Abar = (S + S^T) / 2
 //
-// Every product runs on the tensor cores through gemm_tc.cu (BF16x3 or
-// TF32 operands, FP32 accumulation) with triangular K ranges.  The upper
-// part of Lbar is ignored: tril(L^T triu(Lbar, 1)) = 0.
+// For n > 128 every product runs on the tensor cores through gemm_tc.cu
+// (BF16x3 or TF32 operands, FP32 accumulation) with triangular K ranges.
+// For n <= 128 one CTA per matrix does all of it in shared memory in FP32
+// (bwd_small_kernel), which is both exact to FP32 and one launch instead of
+// eight.  The upper part of Lbar is ignored: tril(L^T triu(Lbar, 1)) = 0.
 //
 // The reference has no backward; the oracle is torch.linalg.cholesky's
 // autograd (same formula) and FP64 finite differences.
@@ -18,6 +20,7 @@
 
 #include "diag64.cuh"
 #include "launch.h"
+#include "tile_engine.cuh"
 
 namespace b2p {
 
@@ -57,6 +60,104 @@ __global__ void sym_kernel(const float* __restrict__ s, float* __restrict__ out,
     const int i = (int)(r / n), j = (int)(r - (int64_t)(r / n) * n);
     const float* sb = s + b * (int64_t)n * n;
     out[e] = 0.5f * (sb[(size_t)i * n + j] + sb[(size_t)j * n + i]);
+  }
+}
+
+// ---- n <= 128: one CTA per matrix ------------------------------------------
+constexpr int kBsThreads = 256;
+constexpr int kBsLd = 132;                      // row stride of the three 128x128 buffers
+constexpr int kBsBuf = 128 * kBsLd;             // floats per buffer
+constexpr int kBsWork = 4 * 32 * 33;            // smem_trtri's work area
+constexpr size_t kBsSmemBytes = sizeof(float) * (size_t)(3 * kBsBuf + kBsWork + 128 + 4);
+
+// acc[r][c] = sum_{k in [k0, k1)} X[k][8ti + r] * Y[k][8tj + c] (X, Y row-major
+// in shared memory, row stride kBsLd): the X^T Y tile of this thread.
+__device__ __forceinline__ void bs_tile(const float* X, const float* Y, int ti, int tj, int k0, int k1,
+                                        float (&acc)[8][8]) {
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
+#pragma unroll 2
+  for (int k = k0; k < k1; ++k) {
+    const float4 x0 = *reinterpret_cast<const float4*>(X + k * kBsLd + 8 * ti);
+    const float4 x1 = *reinterpret_cast<const float4*>(X + k * kBsLd + 8 * ti + 4);
+    const float4 y0 = *reinterpret_cast<const float4*>(Y + k * kBsLd + 8 * tj);
+    const float4 y1 = *reinterpret_cast<const float4*>(Y + k * kBsLd + 8 * tj + 4);
+    const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+    const float yv[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
+  }
+}
+
+__global__ void __launch_bounds__(kBsThreads, 1)
+    bwd_small_kernel(const float* __restrict__ l, const float* __restrict__ lbar, float* __restrict__ abar,
+                     int64_t batch, int n) {
+  extern __shared__ __align__(16) float bsm[];
+  float* bA = bsm;               // L, later S
+  float* bB = bsm + kBsBuf;      // Lbar, later P^T, later Z
+  float* bC = bsm + 2 * kBsBuf;  // U = L^{-1}
+  float* work = bsm + 3 * kBsBuf;
+  TileScratch sc{};
+  sc.invd = work + kBsWork;
+  const int tid = threadIdx.x;
+  const int ti = tid >> 4, tj = tid & 15;
+  float acc[8][8];
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const float* L = l + (size_t)b * n * n;
+    const float* G = lbar + (size_t)b * n * n;
+    // L (lower, identity beyond n) and Lbar (lower, zero beyond n).
+    for (int e = tid; e < 128 * 128; e += kBsThreads) {
+      const int i = e >> 7, j = e & 127;
+      const bool in = i < n && j < n && j <= i;
+      bA[i * kBsLd + j] = in ? L[(size_t)i * n + j] : (i == j ? 1.0f : 0.0f);
+      bB[i * kBsLd + j] = in ? G[(size_t)i * n + j] : 0.0f;
+    }
+    __syncthreads();
+    if (tid < 128) sc.invd[tid] = 1.0f / bA[tid * kBsLd + tid];
+    // P = Phi(L^T Lbar) (lower tiles; k >= max(i, j)), kept in registers.
+    const bool lower = tj <= ti;
+    if (lower) bs_tile(bA, bB, ti, tj, 8 * ti, 128, acc);
+    __syncthreads();
+    // P^T into bB.
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int i = 8 * ti + r, j = 8 * tj + c;
+        const float v = !lower || j > i ? 0.0f : (j == i ? 0.5f * acc[r][c] : acc[r][c]);
+        bB[j * kBsLd + i] = v;
+      }
+    // U = L^{-1} into bC.
+    smem_trtri<kBsThreads>(bA, 128, kBsLd, bC, kBsLd, sc, work);
+    __syncthreads();
+    // Z = P U: Z[i][j] = sum_k P^T[k][i] U[k][j], k in [j, i] (lower tiles).
+    if (lower) bs_tile(bB, bC, ti, tj, 8 * tj, 8 * ti + 8, acc);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int i = 8 * ti + r, j = 8 * tj + c;
+        bB[i * kBsLd + j] = (lower && j <= i) ? acc[r][c] : 0.0f;
+      }
+    __syncthreads();
+    // S = U^T Z: S[i][j] = sum_k U[k][i] Z[k][j], k >= max(i, j); into bA.
+    bs_tile(bC, bB, ti, tj, 8 * (ti > tj ? ti : tj), 128, acc);
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) bA[(8 * ti + r) * kBsLd + 8 * tj + c] = acc[r][c];
+    __syncthreads();
+    float* Ab = abar + (size_t)b * n * n;
+    for (int e = tid; e < n * n; e += kBsThreads) {
+      const int i = e / n, j = e - (e / n) * n;
+      Ab[e] = 0.5f * (bA[i * kBsLd + j] + bA[j * kBsLd + i]);
+    }
+    __syncthreads();
   }
 }
 
@@ -104,13 +205,23 @@ static int trtri_rec(const float* l, float* u, float* tmp, int64_t batch, int n,
   return launch_gemm_tc(g, mode, err, s);
 }
 
-size_t backward_workspace_bytes(int64_t batch, int64_t n) { return (size_t)2 * batch * n * n * sizeof(float); }
+size_t backward_workspace_bytes(int64_t batch, int64_t n) {
+  return n <= 128 ? 0 : (size_t)2 * batch * n * n * sizeof(float);
+}
 
 int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, int mode, void* ws,
                    size_t ws_bytes, cudaStream_t s) {
   const int m = mode & B2P_MODE_MASK;
   if (m != B2P_MODE_TF32 && m != B2P_MODE_BF16X3)
     return set_error(B2P_ERR_UNSUPPORTED, "backward runs its products in tf32 or bf16x3 (mode 0x%x)", mode);
+  if (n <= 128) {
+    // One CTA per matrix, everything in shared memory, FP32 in every mode.
+    if (int st = ensure_smem_attr((const void*)bwd_small_kernel, kBsSmemBytes, kSlotBwdSmall)) return st;
+    TraceScope ts(kKBwdSym, s);
+    const int grid = (int)std::min<int64_t>(batch, (int64_t)device_sms());
+    bwd_small_kernel<<<grid, kBsThreads, kBsSmemBytes, s>>>(l, lbar, abar, batch, n);
+    return check_launch("bwd_small_kernel");
+  }
   const size_t need = backward_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);

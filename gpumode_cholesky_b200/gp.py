@@ -15,8 +15,11 @@ import torch
 from .autograd import cholesky_differentiable
 
 
-def gp_nll(a: torch.Tensor, y: torch.Tensor, mode: str | int | None = None, bwd_mode: str | int = "bf16x3"):
-    """Per-item loss of a batch: ``a`` (batch, n, n) SPD, ``y`` (batch, n); returns (batch,)."""
+def gp_nll(a: torch.Tensor, y: torch.Tensor, mode: str | int | None = "auto", bwd_mode: str | int = "bf16x3"):
+    """Per-item loss of a batch: ``a`` (batch, n, n) SPD, ``y`` (batch, n); returns (batch,).
+
+    ``mode`` is the forward precision (default "auto": BF16x3 for n > 128).
+    """
     l = cholesky_differentiable(a, mode, bwd_mode)
     alpha = torch.linalg.solve_triangular(l, y.unsqueeze(-1), upper=False).squeeze(-1)
     return 0.5 * (alpha * alpha).sum(-1) + torch.log(torch.diagonal(l, dim1=-2, dim2=-1)).sum(-1)

@@ -37,13 +37,19 @@ def workspace(device: torch.device, nbytes: int) -> torch.Tensor:
 
 
 def resolve_mode(mode: str | int | None, n: int) -> int:
-    """Precision mode code for order n; None picks the library default (FP32)."""
+    """Precision mode code for order n; None picks the library default (FP32).
+
+    "auto" is BF16x3 trailing updates for n > 128 (the mixed form that meets
+    the 1e-5 relative residual) and FP32 below, where no update is blocked.
+    """
     if mode is None:
         return _lib.MODE_FP32
     if isinstance(mode, int):
         return mode
     flags = 0
     name = mode.lower()
+    if name == "auto":
+        return _lib.MODE_BF16X3 if n > 128 else _lib.MODE_FP32
     if name.endswith("+fp64diag"):
         flags = _lib.FLAG_FP64_DIAG
         name = name[: -len("+fp64diag")]

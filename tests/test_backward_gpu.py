@@ -38,7 +38,7 @@ def test_adjoint_matches_golden_autograd(golden_backward, mode):
         assert _rel(abar, g["abar"]) <= TOL[mode], (g["l"].shape, _rel(abar, g["abar"]))
 
 
-@pytest.mark.parametrize("batch,n", [(4, 64), (3, 100), (2, 257), (2, 512)])
+@pytest.mark.parametrize("batch,n", [(5, 17), (4, 64), (3, 100), (2, 127), (2, 257), (2, 512)])
 def test_adjoint_matches_oracle(batch, n):
     a = inputs.well_conditioned(batch, n, seed=n, device="cpu")
     l = cholesky(a.cuda())

@@ -97,6 +97,8 @@ def test_error_raises_python_exception():
 def test_mode_names():
     assert resolve_mode(None, 512) == _lib.MODE_FP32
     assert resolve_mode("bf16x3", 512) == _lib.MODE_BF16X3
+    assert resolve_mode("auto", 512) == _lib.MODE_BF16X3
+    assert resolve_mode("auto", 128) == _lib.MODE_FP32
     assert resolve_mode("tf32+fp64diag", 512) == _lib.MODE_TF32 | _lib.FLAG_FP64_DIAG
     with pytest.raises(ValueError):
         resolve_mode("int8", 512)
