@@ -70,7 +70,7 @@ int ensure_smem_attr(const void* func, size_t bytes, int slot) {
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-static bool path_supported(int path, int64_t batch, int64_t n, int mode) {
+bool path_supported(int path, int64_t batch, int64_t n, int mode) {
   switch (path) {
     case B2P_PATH_BLOCKED: return true;
     case B2P_PATH_FUSED: return fused_supported(n, mode);
@@ -85,19 +85,29 @@ static bool path_supported(int path, int64_t batch, int64_t n, int mode) {
 // the GPU (640x512: 1225 us), else the warp-specialized kernel in clusters of
 // up to 8 CTAs per matrix (60x1024: 646 us, 4x1024: 421 us); above 1024 the
 // multi-CTA split path (8x2048: 1351 us).  FP32: blocked.
-static int choose_path(int64_t batch, int64_t n, int mode) {
+int choose_path(int64_t batch, int64_t n, int mode) {
   const int64_t sms = device_sms();
   if (fused_supported(n, mode)) return batch > sms ? B2P_PATH_FUSED : B2P_PATH_FUSED_WS;
   if (split_supported(n, mode)) return B2P_PATH_SPLIT;
   return B2P_PATH_BLOCKED;
 }
 
-static size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
+size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
   switch (path) {
     case B2P_PATH_FUSED:
     case B2P_PATH_FUSED_WS: return fused_workspace_bytes(batch, n);
     case B2P_PATH_SPLIT: return split_workspace_bytes(batch, n);
     default: return blocked_workspace_bytes(batch, n, mode);
+  }
+}
+
+int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
+               int32_t* info, cudaStream_t s) {
+  switch (path) {
+    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    default: return potrf_blocked(a, l, batch, n, mode, ws, ws_bytes, info, s);
   }
 }
 
@@ -166,12 +176,7 @@ int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, i
   if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
   if (!path_supported(path, batch, n, mode))
     return set_error(B2P_ERR_UNSUPPORTED, "path %d does not support n=%lld mode 0x%x", path, (long long)n, mode);
-  switch (path) {
-    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
-    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
-    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
-    default: return potrf_blocked(a, l, batch, (int)n, mode, workspace, workspace_bytes, info, s);
-  }
+  return potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

@@ -57,6 +57,15 @@ size_t split_workspace_bytes(int64_t batch, int64_t n);
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s);
 
+// The n > 128 dispatcher (capi.cu): the path for (batch, n, mode), whether a
+// path takes a shape, its workspace, and a launch on an explicit path (n > 128;
+// the caller has checked path_supported).
+int choose_path(int64_t batch, int64_t n, int mode);
+bool path_supported(int path, int64_t batch, int64_t n, int mode);
+size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode);
+int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
+               int32_t* info, cudaStream_t s);
+
 // Batched tensor-core GEMM with structure hints (gemm_tc.cu):
 // C = alpha * op1(X) op2(Y) + beta * C per batch item.
 struct GemmArgs {
@@ -92,12 +101,13 @@ enum KernelId {
   kKTrailTc,
   kKSplitStep,
   kKSplitUpdate,
-  kKRagged,
+  kKRaggedGather,
   kKBwdGemm,
   kKBwdTrsm,
   kKBwdSym,
   kKFused,
   kKFusedWs,
+  kKRaggedScatter,
   kKCount
 };
 

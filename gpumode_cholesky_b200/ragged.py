@@ -41,7 +41,13 @@ def unpack(buf: torch.Tensor, orders: Sequence[int], offsets: Sequence[int]) -> 
 
 
 class RaggedPlan:
-    """Schedule for one list of orders (and offsets) on one device."""
+    """Schedule for one list of orders (and offsets) on one device.
+
+    ``tc_min_n`` (tensor modes): matrices of at least this order (and > 128)
+    are factored as identity-padded dense batches, one per padded order
+    (multiple of 64); smaller ones take the blocked ragged schedule.  0 picks
+    the library default (every n > 128 padded).
+    """
 
     def __init__(
         self,

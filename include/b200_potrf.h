@@ -135,13 +135,19 @@ B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, i
  * contiguous n_i*n_i floats; offsets multiples of 4).  The output buffer uses
  * the same offsets.  Usage:
  *   b2p_ragged_plan_create   host-only: buckets the orders and precomputes
- *                            every launch (tc_min_n: in tensor modes, the
- *                            smallest order whose trailing updates use the
- *                            tensor cores; 0 = default 256);
+ *                            every launch.  tc_min_n (tensor modes; 0 =
+ *                            default 129): matrices of at least this order
+ *                            (and > 128) are copied into identity-padded
+ *                            dense batches (order rounded up to 64, one
+ *                            batch per padded order) and factored on the
+ *                            dense tensor-core paths; smaller ones take the
+ *                            blocked ragged schedule;
  *   b2p_ragged_plan_upload   copies the plan's tables (table_bytes, 16-byte
  *                            aligned device buffer) to the device; blocking;
  *   b2p_potrf_ragged         enqueues the factorization; reads only device
  *                            memory, so it can be captured in a CUDA graph;
+ *                            workspace: b2p_ragged_plan_workspace_bytes (holds
+ *                            the padded copies in tensor modes);
  *   b2p_ragged_plan_destroy.
  * info (optional, device int32[count]) follows b2p_potrf_batched.  No
  * counterpart exists in the reference (its dispatcher routes exact

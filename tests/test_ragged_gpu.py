@@ -87,6 +87,57 @@ def test_ragged_nonspd_info():
     assert info.cpu().tolist() == want
 
 
+def _identity_padded(m: torch.Tensor, p: int) -> torch.Tensor:
+    n = m.shape[-1]
+    out = torch.eye(p, dtype=torch.float32)
+    out[:n, :n] = m
+    return out
+
+
+def test_ragged_dense_groups_bitwise_equal_padded_dense():
+    """Tensor modes: a matrix of order n > 128 is factored as its identity-padded
+    copy (order rounded up to 64) in a dense batch of all matrices sharing that
+    padded order, so its factor equals the dense entry point's factor of the
+    padded batch, bit for bit.  The workspace is filled with NaN first: the
+    padded copies must not read anything the gather did not write."""
+    orders = [200, 150, 256, 300, 1000, 1100, 1090, 40]
+    mats = [inputs.generate_input(1, n, 2, 17 + n, "dense", device="cpu")[0] for n in orders]
+    buf, orders, offs = pack(mats, device="cuda")
+    plan = RaggedPlan(orders, offs, mode="bf16x3")
+    plan.workspace.fill_(0xFF)
+    info = torch.full((len(orders),), -5, dtype=torch.int32, device="cuda")
+    out = plan.factor(buf, info=info)
+    torch.cuda.synchronize()
+    assert (info == 0).all()
+    groups: dict[int, list[int]] = {}
+    for i, n in enumerate(orders):
+        if n > 128:
+            groups.setdefault((n + 63) // 64 * 64, []).append(i)
+    ls = unpack(out, orders, offs)
+    for p, idx in groups.items():
+        batch = torch.stack([_identity_padded(mats[i], p) for i in idx]).cuda()
+        dense = cholesky(batch, mode="bf16x3")
+        for j, i in enumerate(idx):
+            n = orders[i]
+            assert torch.equal(ls[i], dense[j, :n, :n]), (n, p)
+            assert torch.equal(dense[j, n:, n:], torch.eye(p - n, device="cuda")), (n, p)
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "tf32", "fp32"])
+def test_ragged_nonspd_info_all_buckets(mode):
+    orders = [20, 70, 190, 300, 640, 1090]
+    mats = [inputs.well_conditioned(1, n, seed=n, device="cpu")[0] for n in orders]
+    bad = {0: 7, 1: 33, 2: 100, 3: 299, 5: 1088}
+    for i, j in bad.items():
+        mats[i][j, j] = -3.0
+    buf, orders, offs = pack(mats, device="cuda")
+    info = torch.full((len(orders),), -5, dtype=torch.int32, device="cuda")
+    RaggedPlan(orders, offs, mode=mode).factor(buf, info=info)
+    want = [int(oracle.potrf_f64(m.unsqueeze(0).double().numpy())[1][0]) for m in mats]
+    assert want[4] == 0 and all(want[i] == j + 1 for i, j in bad.items())
+    assert info.cpu().tolist() == want
+
+
 def test_config4_full_size():
     """3000 matrices, n log-uniform in [16, 2048]: every factor reconstructs its matrix."""
     orders = inputs.ragged_orders(3000, seed=4)

@@ -17,14 +17,41 @@ def _plan(orders, offsets=None, mode=0, tc_min_n=0):
     return st, h
 
 
+def _padded_elems(orders, min_n=129):
+    return sum(((n + 63) // 64 * 64) ** 2 for n in orders if n > 128 and n >= min_n)
+
+
 def test_plan_sizes_and_destroy():
     lib = _lib.load()
     orders = [1, 16, 32, 33, 100, 128, 129, 300, 1000]
     st, h = _plan(orders)
     assert st == _lib.B2P_OK
-    # three big matrices -> one 64x64 inverse slot each
-    assert lib.b2p_ragged_plan_workspace_bytes(h) == 3 * 64 * 64 * 4
+    # FP32: three blocked matrices -> one 64x64 inverse slot each (+ alignment slack)
+    assert lib.b2p_ragged_plan_workspace_bytes(h) == 3 * 64 * 64 * 4 + 1024
     assert lib.b2p_ragged_plan_table_bytes(h) > 8 * len(orders)
+    lib.b2p_ragged_plan_destroy(h)
+
+
+def test_plan_tensor_mode_pads_into_dense_groups():
+    """Tensor modes: n > 128 matrices are padded to multiples of 64 (A and L copies)."""
+    lib = _lib.load()
+    orders = [1, 16, 100, 129, 130, 192, 300, 1000, 1500]
+    st, h = _plan(orders, mode=_lib.MODE_BF16X3)
+    assert st == _lib.B2P_OK
+    ws = lib.b2p_ragged_plan_workspace_bytes(h)
+    assert ws >= 2 * 4 * _padded_elems(orders)
+    tb_dense = lib.b2p_ragged_plan_table_bytes(h)
+    lib.b2p_ragged_plan_destroy(h)
+    # dense_min_n above every order: all big matrices take the blocked schedule
+    st, h = _plan(orders, mode=_lib.MODE_BF16X3, tc_min_n=1 << 16)
+    assert st == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) == 6 * 64 * 64 * 4 + 1024
+    assert lib.b2p_ragged_plan_table_bytes(h) != tb_dense
+    lib.b2p_ragged_plan_destroy(h)
+    # a threshold in between splits them
+    st, h = _plan(orders, mode=_lib.MODE_BF16X3, tc_min_n=300)
+    assert st == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * _padded_elems(orders, 300) + 3 * 64 * 64 * 4
     lib.b2p_ragged_plan_destroy(h)
 
 
@@ -55,9 +82,12 @@ def test_config4_orders_plan():
     lib = _lib.load()
     orders = inputs.ragged_orders(3000, seed=4)
     assert min(orders) >= 16 and max(orders) <= 2048
-    for mode in (0, _lib.MODE_BF16X3):
-        st, h = _plan(orders, mode=mode)
-        assert st == _lib.B2P_OK
-        big = sum(1 for n in orders if n > 128)
-        assert lib.b2p_ragged_plan_workspace_bytes(h) == big * 64 * 64 * 4
-        lib.b2p_ragged_plan_destroy(h)
+    big = sum(1 for n in orders if n > 128)
+    st, h = _plan(orders, mode=0)
+    assert st == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) == big * 64 * 64 * 4 + 1024
+    lib.b2p_ragged_plan_destroy(h)
+    st, h = _plan(orders, mode=_lib.MODE_BF16X3)
+    assert st == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * _padded_elems(orders)
+    lib.b2p_ragged_plan_destroy(h)
