@@ -29,6 +29,17 @@ MODES = {"fp32": MODE_FP32, "tf32": MODE_TF32, "bf16x3": MODE_BF16X3, "fp8": MOD
 
 PATHS = {"auto": 0, "blocked": 1, "fused": 2, "fused_ws": 3, "split": 4}
 
+
+class RaggedOptions(ctypes.Structure):
+    """Mirror of b2p_ragged_options (include/b200_potrf.h); zero = default."""
+
+    _fields_ = [
+        ("dense_min_n", ctypes.c_int32),
+        ("pad_step", ctypes.c_int32),
+        ("pad_step_large", ctypes.c_int32),
+        ("large_path", ctypes.c_int32),
+    ]
+
 # Every symbol the header declares, with (restype, argtypes).
 _c_i64 = ctypes.c_int64
 _c_sz = ctypes.c_size_t
@@ -50,6 +61,7 @@ SIGNATURES = {
     "b2p_noalloc_scratch_bytes": (_c_sz, []),
     "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_ragged_plan_create": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, ctypes.c_int, _c_p]),
+    "b2p_ragged_plan_create_ex": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_ragged_plan_destroy": (None, [_c_p]),
     "b2p_ragged_plan_table_bytes": (_c_sz, [_c_p]),
     "b2p_ragged_plan_workspace_bytes": (_c_sz, [_c_p]),

@@ -46,8 +46,10 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
 // per matrix for small batches: same workspace and contract.
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                    int32_t* info, cudaStream_t s);
-// Orders and batches the warp-specialized kernel can take (n <= 8192; for
-// n > 1024 the batch must leave room for clusters large enough for TMEM).
+// Orders and batches the warp-specialized kernel can take (n <= 8192, in
+// clusters large enough for TMEM), and the subset the dispatcher and the
+// forced-path entry point offer (n <= 1024).
+bool fused_ws_fits(int64_t batch, int64_t n, int mode);
 bool fused_ws_supported(int64_t batch, int64_t n, int mode);
 
 // Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
@@ -108,6 +110,7 @@ enum KernelId {
   kKFused,
   kKFusedWs,
   kKRaggedScatter,
+  kKSplitWide,
   kKCount
 };
 
@@ -154,6 +157,8 @@ enum SmemSlot {
   kSlotSplitU1,
   kSlotSplitS0,
   kSlotSplitS1,
+  kSlotSplitW0,
+  kSlotSplitW1,
   kSlotBwdSmall,
   kSlotCount
 };

@@ -61,26 +61,28 @@ __device__ __forceinline__ void panel_copy_store(uint8_t* w0, uint8_t* w1, int N
   }
 }
 
-// D (128 x 64 FP32 in TMEM) (+)= A B^T over one 64-wide column, from staged
-// copies: A = 128 rows at sa (region 0 at +0, region 1 at +16384), B = 64
-// rows at sb (region 0 at +0, region 1 at +8192).  One thread issues.
-template <int MODE>
+// D (128 x NB FP32 in TMEM) (+)= A B^T over one 64-wide column, from staged
+// copies: A = 128 rows at sa (region 0 at +0, region 1 at +16384), B = NB
+// rows at sb (region 0 at +0, region 1 at +128 NB).  One thread issues.
+template <int MODE, int NB = 64>
 __device__ __forceinline__ void panel_copy_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
+  static_assert(NB % 16 == 0 && NB >= 16 && NB <= 256, "MMA N for M = 128");
+  constexpr uint32_t kB1 = 128u * NB;
   if (MODE == B2P_MODE_TF32) {
-    constexpr uint32_t idesc = umma::idesc_f32acc(2, 128, 64);
+    constexpr uint32_t idesc = umma::idesc_f32acc(2, 128, NB);
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
       const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
-      const uint32_t kb = (uint32_t)((s >> 2) * 8192 + (s & 3) * 32);
+      const uint32_t kb = (uint32_t)((s >> 2) * kB1 + (s & 3) * 32);
       umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
     }
   } else {
-    constexpr uint32_t idesc = umma::idesc_f32acc(1, 128, 64);
+    constexpr uint32_t idesc = umma::idesc_f32acc(1, 128, NB);
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const uint32_t o = (uint32_t)(s * 32);
       const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
-      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + 8192 + o);
+      const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + kB1 + o);
       umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
       umma::mma_bf16(d, ah, bl, idesc, 1u);
       umma::mma_bf16(d, ah, bh, idesc, 1u);

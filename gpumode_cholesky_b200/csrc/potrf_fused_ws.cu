@@ -453,11 +453,13 @@ static int ws_cluster_size(int64_t batch, int n) {
 // but with K up to n every CTA then streams its whole row range of panel
 // copies per block column and is bound by its own bulk-copy bandwidth
 // (8x2048: 1630 us against 1351 us on the split path; 1x4096: 7490 vs 2335).
-bool fused_ws_supported(int64_t batch, int64_t n, int mode) {
+bool fused_ws_fits(int64_t batch, int64_t n, int mode) {
   const int m = mode & B2P_MODE_MASK;
   return (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3) && !(mode & B2P_FLAG_FP64_DIAG) && n > 128 && n % 64 == 0 &&
-         n <= 1024 && ws_cluster_size(batch, (int)n) > 0;
+         n <= 8192 && ws_cluster_size(batch, (int)n) > 0;
 }
+
+bool fused_ws_supported(int64_t batch, int64_t n, int mode) { return n <= 1024 && fused_ws_fits(batch, n, mode); }
 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                    int32_t* info, cudaStream_t s) {
@@ -467,7 +469,7 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   uint8_t* wsa = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(ws) + 1023) & ~(uintptr_t)1023);
   const int64_t sms = device_sms();
   const int cl = ws_cluster_size(batch, n);
-  if (cl == 0 || !fused_ws_supported(batch, n, mode))
+  if (cl == 0 || !fused_ws_fits(batch, n, mode))
     return set_error(B2P_ERR_UNSUPPORTED, "warp-specialized path: n=%d not supported", n);
   const int grid = cl * (int)std::max<int64_t>(1, std::min<int64_t>(batch, sms / cl));
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;

@@ -154,8 +154,23 @@ extern "C" {
 
 int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, int64_t count, int mode,
                            int tc_min_n, b2p_ragged_plan** plan_out) {
+  b2p_ragged_options opt = {};
+  opt.dense_min_n = tc_min_n;
+  return b2p_ragged_plan_create_ex(offsets_host, n_host, count, mode, &opt, plan_out);
+}
+
+int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host, int64_t count, int mode,
+                              const b2p_ragged_options* options, b2p_ragged_plan** plan_out) {
   if (plan_out == nullptr) return set_error(B2P_ERR_INVALID_ARG, "null plan pointer");
   *plan_out = nullptr;
+  b2p_ragged_options opt = {};
+  if (options != nullptr) opt = *options;
+  auto step_ok = [](int v) { return v == 0 || v == 64 || v == 128 || v == 256; };
+  if (opt.dense_min_n < 0 || !step_ok(opt.pad_step) || !step_ok(opt.pad_step_large) ||
+      (opt.large_path != B2P_PATH_AUTO && opt.large_path != B2P_PATH_SPLIT && opt.large_path != B2P_PATH_FUSED_WS))
+    return set_error(B2P_ERR_INVALID_ARG, "bad ragged options (pad steps 64/128/256; large path auto/split/fused_ws)");
+  const int step_small = opt.pad_step ? opt.pad_step : kPadStep;
+  const int step_large = opt.pad_step_large ? opt.pad_step_large : kPadStep;
   if (count < 0 || (count > 0 && (offsets_host == nullptr || n_host == nullptr)))
     return set_error(B2P_ERR_INVALID_ARG, "bad ragged list");
   const int m = mode & B2P_MODE_MASK;
@@ -168,7 +183,7 @@ int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, i
   if (plan == nullptr) return set_error(B2P_ERR_INVALID_ARG, "out of host memory");
   RaggedPlanImpl& p = plan->impl;
   p.mode = mode;
-  p.dense_min_n = tc_min_n > 0 ? tc_min_n : kDefaultDenseMinN;
+  p.dense_min_n = opt.dense_min_n > 0 ? opt.dense_min_n : kDefaultDenseMinN;
   p.count = count;
   std::vector<int32_t> small, mid, big, dense;
   for (int64_t i = 0; i < count; ++i) {
@@ -235,7 +250,11 @@ int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, i
   }
   // Padded dense groups: by padded order, largest first.
   std::map<int, std::vector<int32_t>, std::greater<int>> by_p;
-  for (int32_t i : dense) by_p[(n_host[i] + kPadStep - 1) / kPadStep * kPadStep].push_back(i);
+  for (int32_t i : dense) {
+    const int n = n_host[i];
+    const int step = n > 1024 ? step_large : step_small;
+    by_p[(n + step - 1) / step * step].push_back(i);
+  }
   std::vector<DenseEntry> dents;
   std::vector<int2> ditems;
   int64_t elem = 0;
@@ -246,7 +265,11 @@ int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, i
     g.count = (int64_t)kv.second.size();
     g.elem = elem;
     g.path = choose_path(g.count, g.p, mode);
-    if (!path_supported(g.path, g.count, g.p, mode)) {
+    if (g.p > 1024 && opt.large_path == B2P_PATH_FUSED_WS && fused_ws_fits(g.count, g.p, mode))
+      g.path = B2P_PATH_FUSED_WS;
+    const bool ok = g.path == B2P_PATH_FUSED_WS ? fused_ws_fits(g.count, g.p, mode)
+                                                 : path_supported(g.path, g.count, g.p, mode);
+    if (!ok) {
       delete plan;
       return set_error(B2P_ERR_UNSUPPORTED, "no dense path for %lld matrices of padded order %d",
                        (long long)g.count, g.p);

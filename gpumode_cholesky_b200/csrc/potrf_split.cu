@@ -27,6 +27,12 @@
 //       and the panel copy of X.  CTA 0 of the matrix writes L_kk and info;
 //       the zero strip right of the diagonal block goes out as bulk stores.
 //
+//   split_wide_kernel       (n >= kWideMinN) the panels older than the
+//       previous 512-column outer block, applied to a whole outer block at
+//       once as 128 x 256 tensor-core tiles on a third stream, so that the
+//       per-column look-ahead only applies the last 8-15 panels (see the
+//       schedule above potrf_split).
+//
 // A is read once and L written once; the panel copies (4 bytes per element
 // in either mode) are the only re-read data and mostly hit L2.  Results are
 // deterministic (the split of each update is fixed by the shapes).  All waits are bounded; a timeout marks the matrix with
@@ -206,6 +212,258 @@ __global__ void __launch_bounds__(kUThreads, 2)
   if (!got) umma::mbar_wait_bounded(done, 0u, kSplitPolls);
   umma::fence_after_sync();
   if (warp == 0) umma::tmem_dealloc(tmem, kUTmemCols);
+}
+
+// ---- wide update kernel ----------------------------------------------------------
+// For large orders the panels older than the previous outer block (kWideCols
+// block columns) are applied to a whole outer block at once:
+//   Out[r, j] = base[r, j] - sum_{c in [c_begin, c_end)} L_c[r] L_c[j0 + j]^T,
+//   rows r >= j0, columns j < nbw,
+// as 128 x 256 tiles (MMA N = 256: each A tile of the panel copies feeds 256
+// output columns instead of 64, which is what makes the update bandwidth
+// affordable at n >= 8192).  item = (matrix, row tile, column tile).
+//
+// Warp roles: warp 8 (one thread) streams the panel copies through a
+// two-stage ring of bulk copies and issues the MMAs; warps 0-7 own the
+// accumulator.  The tensor core adds into its FP32 accumulator without
+// round-to-nearest, and over K = n that bias grows with n; so the MMAs of
+// every kXChunk panels go into one of two TMEM accumulators (ping-pong), and
+// the consumer warps fold each finished one into FP32 registers (warp w:
+// TMEM lanes 32 (w % 4) .., columns 128 (w / 4) ..) while the tensor core
+// fills the other.
+// With segs == 1 every CTA loops over items (a persistent grid, so the step
+// kernels keep the other SMs); with segs > 1 each cluster of segs CTAs
+// splits one item's K range and reduces over distributed shared memory in a
+// fixed order.
+constexpr int kXConsumers = 256;
+constexpr int kXThreads = kXConsumers + 32;
+constexpr int kXCols = 256;
+constexpr int kXChunk = 4;                                    // panels per TMEM accumulation
+constexpr uint32_t kXStageA = 32768;                          // 128 rows x 2 regions
+constexpr uint32_t kXStage = kXStageA + 2u * kXCols * 128u;   // + 256 rows x 2 regions
+constexpr uint32_t kXStaging = 2 * kXStage;
+constexpr int kXParkLd = kXCols + 4;
+constexpr uint32_t kXSmemBytes = kXStaging + 128 + 1024;
+constexpr uint32_t kXTmemCols = 2 * kXCols;
+static_assert(128 * kXParkLd * 4 <= kXStaging, "parked accumulator must fit the staging area");
+
+template <int MODE>
+__global__ void __launch_bounds__(kXThreads, 1)
+    split_wide_kernel(const float* base, int64_t base_mstride, int base_ld, const uint8_t* __restrict__ ws,
+                      float* out, int64_t out_mstride, int out_ld, int64_t batch, int n, int j0, int nbw,
+                      int c_begin, int c_end, int segs, int32_t* __restrict__ info) {
+  extern __shared__ unsigned char xraw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(xraw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + kXStaging);  // [2] stage loaded
+  uint64_t* empty = full + 2;                                     // [2] stage read by its MMAs
+  uint64_t* accf = full + 4;                                      // [2] accumulator complete
+  uint64_t* accd = full + 6;                                      // [2] accumulator folded
+  uint64_t* fin = full + 8;                                       // [1] every MMA done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kXStaging + 80);
+  volatile int* flag = reinterpret_cast<volatile int*>(sm + kXStaging + 84);
+  float* park = reinterpret_cast<float*>(sm);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = n / 64;
+  const size_t rbytes = panel_copy_region_bytes(n);
+  const int s = segs > 1 ? (int)umma::cluster_rank() : 0;
+  const int64_t ncl = gridDim.x / segs;
+  const int rt = (n - j0 + 127) / 128, ct = (nbw + kXCols - 1) / kXCols;
+  const int64_t items = batch * rt * ct;
+  const int span = c_end - c_begin;
+  const int c_lo = c_begin + s * span / segs, c_hi = c_begin + (s + 1) * span / segs;
+  const int iters = c_hi - c_lo;
+  const int nch = (iters + kXChunk - 1) / kXChunk;
+
+  if (tid == 0) *flag = 0;
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kXTmemCols);
+    umma::tmem_relinquish();
+  }
+  if (tid == 32) {
+    for (int i = 0; i < 4; ++i) umma::mbar_init(full + i, 1);   // full, empty
+    for (int i = 4; i < 6; ++i) umma::mbar_init(full + i, 1);   // accf
+    for (int i = 6; i < 8; ++i) umma::mbar_init(full + i, kXConsumers / 32);  // accd
+    umma::mbar_init(fin, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+
+  if (warp == kXConsumers / 32) {
+    // ---------------- producer / MMA issuer ----------------
+    if (lane == 0) {
+      int64_t gi = 0, loaded = 0;  // panels consumed / loaded (all items)
+      int64_t gc = 0;              // chunks started
+      bool ok = true;
+      for (int64_t item = blockIdx.x / segs; item < items && ok; item += ncl) {
+        const int tj = (int)(item % ct);
+        const int ti = (int)((item / ct) % rt);
+        const int64_t b = item / ((int64_t)ct * rt);
+        const int r0 = j0 + 128 * ti, vr = min(128, n - r0);
+        const int cj = kXCols * tj, vc = min(kXCols, nbw - cj);
+        const uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
+        const uint8_t* W1 = W0 + rbytes;
+        // Panel i of this item into its ring stage (after the MMAs of the
+        // panel two before it, which read that stage, have completed).
+        auto load = [&](int i) -> bool {
+          const int64_t g = loaded;
+          const int st = (int)(g & 1);
+          if (g >= 2 && !umma::mbar_wait_bounded(empty + st, (uint32_t)(((g - 2) >> 1) & 1), kSplitPolls))
+            return false;
+          const int c = c_lo + i;
+          const uint32_t abytes = (uint32_t)vr * 128u, bbytes = (uint32_t)vc * 128u;
+          const size_t aoff = panel_copy_row_byte(N, c, r0);
+          const size_t boff = panel_copy_row_byte(N, c, j0 + cj);
+          uint8_t* dst = sm + st * kXStage;
+          umma::mbar_arrive_expect_tx(full + st, 2 * abytes + 2 * bbytes);
+          umma::bulk_g2s(dst, W0 + aoff, abytes, full + st);
+          umma::bulk_g2s(dst + 16384, W1 + aoff, abytes, full + st);
+          umma::bulk_g2s(dst + kXStageA, W0 + boff, bbytes, full + st);
+          umma::bulk_g2s(dst + kXStageA + kXCols * 128, W1 + boff, bbytes, full + st);
+          ++loaded;
+          return true;
+        };
+        if (!load(0)) {
+          ok = false;
+          break;
+        }
+        for (int ch = 0; ch < nch && ok; ++ch, ++gc) {
+          const int p = (int)(gc & 1);
+          // Accumulator p is free once the consumers folded chunk gc - 2.
+          if (gc >= 2 && !umma::mbar_wait_bounded(accd + p, (uint32_t)(((gc - 2) >> 1) & 1), kSplitPolls)) {
+            ok = false;
+            break;
+          }
+          umma::fence_after_sync();
+          const int i_end = min(iters, (ch + 1) * kXChunk);
+          for (int i = ch * kXChunk; i < i_end; ++i, ++gi) {
+            if (i + 1 < iters && !load(i + 1)) {
+              ok = false;
+              break;
+            }
+            const int st = (int)(gi & 1);
+            if (!umma::mbar_wait_bounded(full + st, (uint32_t)((gi >> 1) & 1), kSplitPolls)) {
+              ok = false;
+              break;
+            }
+            umma::fence_after_sync();
+            const uint32_t sa = umma::smem_u32(sm + st * kXStage);
+            panel_copy_mmas<MODE, kXCols>(tmem + (uint32_t)(p * kXCols), sa, sa + kXStageA, i > ch * kXChunk);
+            umma::mma_commit(empty + st);
+          }
+          if (ok) umma::mma_commit(accf + p);
+        }
+      }
+      if (!ok) {
+        // Copies still in flight land before anything leaves.
+        for (int64_t g = gi; g < loaded; ++g) umma::mbar_wait_bounded(full + (g & 1), (uint32_t)((g >> 1) & 1), kSplitPolls);
+        *flag = 1;
+      }
+      umma::mma_commit(fin);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- consumers: fold the accumulators, write Out ----------------
+    const int q = warp & 3, hh = warp >> 2;
+    const int rl = 32 * q + lane;
+    int64_t gc = 0;
+    for (int64_t item = blockIdx.x / segs; item < items; item += ncl) {
+      const int tj = (int)(item % ct);
+      const int ti = (int)((item / ct) % rt);
+      const int64_t b = item / ((int64_t)ct * rt);
+      const int r0 = j0 + 128 * ti, vr = min(128, n - r0);
+      const int cj = kXCols * tj, vc = min(kXCols, nbw - cj);
+      float acc[128];
+#pragma unroll
+      for (int c = 0; c < 128; ++c) acc[c] = 0.0f;
+      bool ok = true;
+      for (int ch = 0; ch < nch; ++ch, ++gc) {
+        const int p = (int)(gc & 1);
+        const bool got = umma::mbar_wait_bounded(accf + p, (uint32_t)((gc >> 1) & 1), kSplitPolls) && *flag == 0;
+        if (!__all_sync(0xffffffffu, got)) {
+          ok = false;
+          break;
+        }
+        umma::fence_after_sync();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          float d[32];
+          umma::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(p * kXCols + 128 * hh + 32 * j), d);
+#pragma unroll
+          for (int c = 0; c < 32; ++c) acc[32 * j + c] += d[c];
+        }
+        umma::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) umma::mbar_arrive(accd + p);
+      }
+      if (!ok) {
+        *flag = 1;
+        if (lane == 0 && info != nullptr) info[b] = -1;
+        break;
+      }
+      const float* B = base + (size_t)b * base_mstride;
+      float* O = out + (size_t)b * out_mstride;
+      const int c0 = 128 * hh;
+      if (segs == 1) {
+        if (rl < vr && c0 < vc) {
+          const float4* src = reinterpret_cast<const float4*>(B + (size_t)(r0 + rl) * base_ld + cj + c0);
+          float4* dst = reinterpret_cast<float4*>(O + (size_t)(r0 + rl) * out_ld + cj + c0);
+#pragma unroll
+          for (int c4 = 0; c4 < 32; ++c4) {
+            if (4 * c4 < vc - c0) {
+              const float4 v = src[c4];
+              dst[c4] = make_float4(v.x - acc[4 * c4], v.y - acc[4 * c4 + 1], v.z - acc[4 * c4 + 2],
+                                    v.w - acc[4 * c4 + 3]);
+            }
+          }
+        }
+      } else {
+        // One item per cluster: every copy into the staging area has landed
+        // (all were read by MMAs), so it takes the parked accumulator.
+#pragma unroll
+        for (int c4 = 0; c4 < 32; ++c4)
+          *reinterpret_cast<float4*>(park + rl * kXParkLd + c0 + 4 * c4) =
+              make_float4(acc[4 * c4], acc[4 * c4 + 1], acc[4 * c4 + 2], acc[4 * c4 + 3]);
+      }
+    }
+  }
+  if (segs > 1) {
+    // Sum the parked accumulators of the cluster in segment order.
+    umma::cluster_sync();
+    const int64_t item = blockIdx.x / segs;
+    if (*flag == 0 && item < items) {
+      const int tj = (int)(item % ct);
+      const int ti = (int)((item / ct) % rt);
+      const int64_t b = item / ((int64_t)ct * rt);
+      const int r0 = j0 + 128 * ti, vr = min(128, n - r0);
+      const int cj = kXCols * tj, vc = min(kXCols, nbw - cj);
+      const float* B = base + (size_t)b * base_mstride;
+      float* O = out + (size_t)b * out_mstride;
+      const int c4n = vc / 4;
+      for (int e = s * kXThreads + tid; e < vr * c4n; e += segs * kXThreads) {
+        const int row = e / c4n, c4 = (e - row * c4n) * 4;
+        float4 v = *reinterpret_cast<const float4*>(B + (size_t)(r0 + row) * base_ld + cj + c4);
+        for (int qq = 0; qq < segs; ++qq) {
+          const float4 u = umma::ld_cluster_f4(park + row * kXParkLd + c4, (uint32_t)qq);
+          v.x -= u.x;
+          v.y -= u.y;
+          v.z -= u.z;
+          v.w -= u.w;
+        }
+        *reinterpret_cast<float4*>(O + (size_t)(r0 + row) * out_ld + cj + c4) = v;
+      }
+    }
+    // No CTA leaves while another may still read its park.
+    umma::cluster_sync();
+  }
+  // Every MMA has completed before TMEM is released.
+  umma::mbar_wait_bounded(fin, 0u, kSplitPolls);
+  umma::fence_after_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kXTmemCols);
 }
 
 // ---- step kernel -------------------------------------------------------------
@@ -440,10 +698,20 @@ bool split_supported(int64_t n, int mode) {
          (n % 64) == 0 && n <= 65536;
 }
 
+// Orders from which the older panels are applied an outer block at a time
+// (split_wide_kernel), and the outer block width in block columns.  At
+// 1 x 8192 the wide stage does not pay yet (3681 us against 3628 us).
+constexpr int kWideMinN = 12288;
+constexpr int kWideCols = 8;  // 512 columns
+static_assert(64 * kWideCols % kXCols == 0, "outer blocks are whole wide tiles");
+
 // Panel copies, then two per-matrix FP32 panel buffers (n x 64 each; block
-// columns alternate between them).
+// columns alternate between them), then for large orders two per-matrix
+// outer-block buffers (n x 512 each, alternating by outer block).
 size_t split_workspace_bytes(int64_t batch, int64_t n) {
-  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 2 * (size_t)batch * n * 64 * sizeof(float) + 1024;
+  size_t bytes = (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 2 * (size_t)batch * n * 64 * sizeof(float);
+  if (n >= kWideMinN) bytes += 2 * (size_t)batch * n * 64 * kWideCols * sizeof(float);
+  return bytes + 1024;
 }
 
 namespace {
@@ -453,6 +721,10 @@ struct SideStream {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[2] = {nullptr, nullptr};
+  // Large orders: the outer-block updates run on a third stream.
+  cudaStream_t wide = nullptr;
+  cudaEvent_t wide_done[2] = {nullptr, nullptr};
+  cudaEvent_t wide_free[2] = {nullptr, nullptr};
 };
 constexpr int kSideDevices = 64;
 SideStream g_side[kSideDevices];
@@ -469,6 +741,11 @@ int side_stream(SideStream** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[0], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[1], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ss.wide, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+      e = cudaEventCreateWithFlags(&ss.wide_done[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.wide_free[i], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "side stream set-up: %s", cudaGetErrorString(e));
   }
   *out = &ss;
@@ -484,6 +761,19 @@ int side_stream(SideStream** out) {
 //   side:                look-ahead(j+2) over panels 0..j
 // step(j) waits for look-ahead(j) (join event j % 2).  Column j uses panel
 // buffer j % 2, which look-ahead(j+2) may only overwrite after step(j).
+//
+// Large orders (n >= kWideMinN) split the look-ahead further.  With outer
+// blocks of W = kWideCols block columns, the panels older than the previous
+// outer block are final a whole outer block before they are needed: right
+// after the last step of outer block J-2, the wide stream computes
+//   Bw_J = A[:, block J] - (panels 0 .. (J-1) W - 1) applied to block J
+// (split_wide_kernel, buffer J % 2), and the look-ahead of a column j in
+// block J >= 2 then starts from Bw_J and applies only the panels
+// (J-1) W .. j-2 (fewer than 2 W).  The first look-ahead of block J waits
+// for Bw_J (event wide_done[J % 2]); Bw_{J+2} waits until the last
+// look-ahead of block J has read buffer J % 2 (event wide_free[J % 2]).  The
+// wide kernel keeps to a bounded number of SMs so that the steps, which
+// carry the critical path, always find free ones.
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s) {
   const size_t need = split_workspace_bytes(batch, n);
@@ -499,10 +789,26 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
   auto upd = tf32 ? split_update_kernel<B2P_MODE_TF32> : split_update_kernel<B2P_MODE_BF16X3>;
   auto stp = tf32 ? split_step_kernel<B2P_MODE_TF32> : split_step_kernel<B2P_MODE_BF16X3>;
+  auto wdk = tf32 ? split_wide_kernel<B2P_MODE_TF32> : split_wide_kernel<B2P_MODE_BF16X3>;
   if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, tf32 ? kSlotSplitU0 : kSlotSplitU1)) return st;
   if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, tf32 ? kSlotSplitS0 : kSlotSplitS1)) return st;
   const int N = n / 64;
   const int64_t n2 = (int64_t)n * n;
+  const bool wide = n >= kWideMinN;
+  constexpr int W = kWideCols;
+  const int nbw = 64 * W;
+  float* bw[2] = {nullptr, nullptr};
+  if (wide) {
+    if (int st = ensure_smem_attr((const void*)wdk, kXSmemBytes, tf32 ? kSlotSplitW0 : kSlotSplitW1)) return st;
+    bw[0] = pb[1] + (size_t)batch * n * 64;
+    bw[1] = bw[0] + (size_t)batch * n * nbw;
+  }
+  // SMs the wide kernel may hold at once.
+  // SMs the wide kernel may hold at once: half while the chain of steps
+  // bounds the time (1 x 16384: 11.6 ms at 74 of 148 SMs, 15.3 ms at 40);
+  // two thirds once the outer-block updates do (1 x 32768: 56.0 ms at 100,
+  // 63.5 ms at 74).
+  const int64_t wide_ctas = std::max<int64_t>(1, n >= 24576 ? sms * 2 / 3 : sms / 2);
 
   // Update of column k over panels [c0, c1) on stream `st`: P = base - sum,
   // split into about per_sm CTAs per SM.
@@ -530,39 +836,97 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_update_kernel: %s", cudaGetErrorString(e));
     return B2P_OK;
   };
-  // Step CTAs of column k (one per SM).
-  auto step_ctas = [&](int k) -> int64_t {
-    const int chunks = (n - 64 * k - 64 + kSThreads - 1) / kSThreads;
-    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), sms / batch));
-    return std::min<int64_t>(batch * G, sms);
+  // Outer-block update of block J (J >= 2) on the wide stream.
+  auto launch_wide = [&](int J) -> int {
+    const int j0 = J * nbw;
+    const int cols = std::min(nbw, n - j0);
+    const int c1 = (J - 1) * W;
+    const int64_t items = batch * ((n - j0 + 127) / 128) * ((cols + kXCols - 1) / kXCols);
+    int segs = 1;
+    int64_t grid = std::min<int64_t>(items, wide_ctas);
+    if (items * 2 <= wide_ctas) {
+      segs = (int)std::max<int64_t>(1, std::min<int64_t>({wide_ctas / items, (int64_t)kSplitSegCap, (int64_t)c1}));
+      grid = items * segs;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(kXThreads, 1, 1);
+    cfg.dynamicSmemBytes = kXSmemBytes;
+    cfg.stream = side->wide;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)segs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TraceScope ts(kKSplitWide, side->wide);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, wdk, (const float*)(a + j0), n2, n, (const uint8_t*)copies,
+                                             bw[J & 1], (int64_t)n * nbw, nbw, batch, n, j0, cols, 0, c1, segs, info);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_wide_kernel: %s", cudaGetErrorString(e));
+    return B2P_OK;
   };
+  // Step CTAs of column k: one per SM, or per SM the wide kernel leaves free.
+  const int64_t step_sms = wide ? sms - wide_ctas : sms;
+  auto step_G = [&](int k) -> int {
+    const int chunks = (n - 64 * k - 64 + kSThreads - 1) / kSThreads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), step_sms / batch));
+  };
+  auto step_ctas = [&](int k) -> int64_t { return std::min<int64_t>(batch * step_G(k), step_sms); };
   auto check = [](cudaError_t e, const char* what) -> int {
     return e == cudaSuccess ? B2P_OK : set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   };
 
   for (int k = 0; k < N; ++k) {
-    const int k0 = 64 * k;
     float* pk = pb[k & 1];
     // Column k >= 2 reads the look-ahead result (panels 0..k-2) from pk.
     if (k >= 2) {
       if (int st = check(cudaStreamWaitEvent(s, side->join[k & 1], 0), "cudaStreamWaitEvent")) return st;
     }
     // Step (with the newest panel k-1): one CTA per SM in total.
-    const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
-    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), sms / batch));
+    const int G = step_G(k);
     const int grid = (int)step_ctas(k);
     {
       TraceScope ts(kKSplitStep, s);
       stp<<<grid, kSThreads, kSSmemBytes, s>>>(a, l, copies, pk, batch, n, k, G, info);
       if (int st = check_launch("split_step_kernel")) return st;
     }
+    // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,
+    // which are all final once step k, the last of block J - 2, is done.
+    const int Jw = (k + 1) / W + 1;
+    const bool start_wide = wide && (k + 1) % W == 0 && Jw >= 2 && Jw * W < N;
+    if (k + 2 < N || start_wide) {
+      if (int st = check(cudaEventRecord(side->fork, s), "cudaEventRecord")) return st;
+    }
+    if (start_wide) {
+      if (int st = check(cudaStreamWaitEvent(side->wide, side->fork, 0), "cudaStreamWaitEvent")) return st;
+      if (Jw >= 4) {
+        if (int st = check(cudaStreamWaitEvent(side->wide, side->wide_free[Jw & 1], 0), "cudaStreamWaitEvent"))
+          return st;
+      }
+      if (int st = launch_wide(Jw)) return st;
+      if (int st = check(cudaEventRecord(side->wide_done[Jw & 1], side->wide), "cudaEventRecord")) return st;
+    }
     // Look-ahead for column k + 2 over panels 0..k (all final now), beside
     // step k + 1.  About one CTA per SM: two of its CTAs fit on an SM, so the
     // scheduler leaves SMs free for the step.
     if (k + 2 < N) {
-      if (int st = check(cudaEventRecord(side->fork, s), "cudaEventRecord")) return st;
       if (int st = check(cudaStreamWaitEvent(side->stream, side->fork, 0), "cudaStreamWaitEvent")) return st;
-      if (int st = launch_update(k + 2, 0, k + 1, a + 64 * (k + 2), n2, n, pb[k & 1], side->stream, 1)) return st;
+      const int j = k + 2, J = j / W;
+      if (wide && J >= 2) {
+        if (j == J * W) {
+          if (int st = check(cudaStreamWaitEvent(side->stream, side->wide_done[J & 1], 0), "cudaStreamWaitEvent"))
+            return st;
+        }
+        if (int st = launch_update(j, (J - 1) * W, k + 1, bw[J & 1] + 64 * (j - J * W), (int64_t)n * nbw, nbw,
+                                   pb[k & 1], side->stream, 1))
+          return st;
+        if (j == std::min(J * W + W, N) - 1) {
+          if (int st = check(cudaEventRecord(side->wide_free[J & 1], side->stream), "cudaEventRecord")) return st;
+        }
+      } else {
+        if (int st = launch_update(j, 0, k + 1, a + 64 * j, n2, n, pb[k & 1], side->stream, 1)) return st;
+      }
       if (int st = check(cudaEventRecord(side->join[k & 1], side->stream), "cudaEventRecord")) return st;
     }
   }

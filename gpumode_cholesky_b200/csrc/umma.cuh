@@ -130,6 +130,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
   return false;
 }
 
+// Arrive (release, CTA scope) on a local mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
 // ---- thread-block clusters ---------------------------------------------------
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;

@@ -45,8 +45,11 @@ class RaggedPlan:
 
     ``tc_min_n`` (tensor modes): matrices of at least this order (and > 128)
     are factored as identity-padded dense batches, one per padded order
-    (multiple of 64); smaller ones take the blocked ragged schedule.  0 picks
-    the library default (every n > 128 padded).
+    (multiple of ``pad_step``, or ``pad_step_large`` above 1024: 64, 128 or
+    256); smaller ones take the blocked ragged schedule.  ``large_path``
+    picks the algorithm of the groups above 1024 ("split" or "fused_ws").
+    Zero / "auto" take the library defaults (every n > 128 padded to a
+    multiple of 64; split above 1024).
     """
 
     def __init__(
@@ -56,6 +59,9 @@ class RaggedPlan:
         mode: str | int | None = None,
         tc_min_n: int = 0,
         device: torch.device | str | None = None,
+        pad_step: int = 0,
+        pad_step_large: int = 0,
+        large_path: str = "auto",
     ):
         self.orders = [int(n) for n in orders]
         self.offsets = [int(o) for o in (offsets if offsets is not None else pack_offsets(self.orders)[:-1])]
@@ -69,9 +75,14 @@ class RaggedPlan:
         offs = (ctypes.c_int64 * max(self.count, 1))(*self.offsets)
         ns = (ctypes.c_int32 * max(self.count, 1))(*self.orders)
         handle = ctypes.c_void_p()
+        if large_path not in ("auto", "split", "fused_ws"):
+            raise ValueError(f"large_path must be auto, split or fused_ws, not {large_path!r}")
+        self.options = _lib.RaggedOptions(int(tc_min_n), int(pad_step), int(pad_step_large), _lib.PATHS[large_path])
         _lib.check(
-            lib.b2p_ragged_plan_create(offs, ns, self.count, self.mode, int(tc_min_n), ctypes.byref(handle)),
-            "b2p_ragged_plan_create",
+            lib.b2p_ragged_plan_create_ex(
+                offs, ns, self.count, self.mode, ctypes.byref(self.options), ctypes.byref(handle)
+            ),
+            "b2p_ragged_plan_create_ex",
         )
         self._handle = handle
         self.table_bytes = lib.b2p_ragged_plan_table_bytes(handle)

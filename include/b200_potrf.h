@@ -156,6 +156,28 @@ B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, i
 typedef struct b2p_ragged_plan b2p_ragged_plan;
 B2P_API int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n_host, int64_t count,
                                    int mode, int tc_min_n, b2p_ragged_plan** plan);
+/*
+ * Tuning knobs of the padded dense groups (tensor modes); zero fields take
+ * the defaults.  b2p_ragged_plan_create(..., tc_min_n, ...) is
+ * b2p_ragged_plan_create_ex with dense_min_n = tc_min_n and the rest zero.
+ *   dense_min_n     as tc_min_n above (default 129)
+ *   pad_step        padded-order granularity for orders <= 1024: 64, 128 or
+ *                   256 (default 64); coarser steps make fewer, larger groups
+ *                   at the cost of padding work
+ *   pad_step_large  the same for orders > 1024 (default 64)
+ *   large_path      path of the groups with padded order > 1024:
+ *                   B2P_PATH_AUTO (= SPLIT), B2P_PATH_SPLIT or
+ *                   B2P_PATH_FUSED_WS (clusters of CTAs per matrix, one
+ *                   launch per group; orders up to 8192)
+ */
+typedef struct b2p_ragged_options {
+  int32_t dense_min_n;
+  int32_t pad_step;
+  int32_t pad_step_large;
+  int32_t large_path;
+} b2p_ragged_options;
+B2P_API int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host, int64_t count,
+                                      int mode, const b2p_ragged_options* options, b2p_ragged_plan** plan);
 B2P_API void b2p_ragged_plan_destroy(b2p_ragged_plan* plan);
 B2P_API size_t b2p_ragged_plan_table_bytes(const b2p_ragged_plan* plan);
 B2P_API size_t b2p_ragged_plan_workspace_bytes(const b2p_ragged_plan* plan);

@@ -56,6 +56,37 @@ def test_split_path(mode, batch, n):
     _check_factor(l, a, mode)
 
 
+@pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("batch,n", [(1, 8192), (2, 12288), (1, 12352)])
+def test_split_path_large_orders(mode, batch, n):
+    """n >= 12288: the panels older than the previous 512-column outer block
+    are applied by the wide update (12352 ends in a partial outer block);
+    8192 runs without it.  Factor bars as above; a negative pivot deep in the
+    matrix gives the oracle's info; the result is bitwise reproducible."""
+    a = torch.stack([inputs.large_gram(n, seed=n + i, device="cuda")[0] for i in range(batch)])
+    info = torch.full((batch,), -9, dtype=torch.int32, device="cuda")
+    l = cholesky(a, mode=mode, info=info, path="split")
+    assert (info == 0).all()
+    assert torch.isfinite(l).all()
+    assert (torch.triu(l, 1) == 0).all()
+    assert (torch.diagonal(l, dim1=-2, dim2=-1) > 0).all()
+    # Above n ~ 1e4 an FP32 factorization itself leaves a relative residual
+    # above 1e-5 (rounding grows like sqrt(n) eps), so BF16x3 is held to
+    # 1e-5 or twice the residual of the FP32 library factor, whichever is larger.
+    bar = TOL_FACTOR[mode]
+    if mode == "bf16x3":
+        bar = max(bar, 2.0 * _residual(torch.linalg.cholesky(a), a))
+    assert _residual(l, a) <= bar
+    again = cholesky(a, mode=mode, path="split")
+    assert torch.equal(l, again)
+    j = n - 700
+    a[batch - 1, j, j] = -1.0
+    cholesky(a, mode=mode, info=info, path="split")
+    assert info[batch - 1].item() == j + 1
+    if batch > 1:
+        assert (info[: batch - 1] == 0).all()
+
+
 @pytest.mark.parametrize("path", ["fused", "fused_ws", "split", "blocked"])
 @pytest.mark.parametrize("mode", ["tf32", "bf16x3"])
 def test_paths_agree(path, mode):

@@ -91,3 +91,36 @@ def test_config4_orders_plan():
     assert st == _lib.B2P_OK
     assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * _padded_elems(orders)
     lib.b2p_ragged_plan_destroy(h)
+
+
+def _plan_ex(orders, mode, **kw):
+    lib = _lib.load()
+    offsets = inputs.pack_offsets(orders)[:-1]
+    offs = (ctypes.c_int64 * max(len(orders), 1))(*offsets)
+    ns = (ctypes.c_int32 * max(len(orders), 1))(*orders)
+    opt = _lib.RaggedOptions(
+        kw.get("dense_min_n", 0), kw.get("pad_step", 0), kw.get("pad_step_large", 0), kw.get("large_path", 0)
+    )
+    h = ctypes.c_void_p()
+    st = lib.b2p_ragged_plan_create_ex(offs, ns, len(orders), mode, ctypes.byref(opt), ctypes.byref(h))
+    return st, h
+
+
+def test_plan_options():
+    lib = _lib.load()
+    orders = [130, 200, 250, 1030, 1500, 2048]
+    st, h = _plan_ex(orders, _lib.MODE_BF16X3, pad_step=256, pad_step_large=256, large_path=_lib.PATHS["fused_ws"])
+    assert st == _lib.B2P_OK
+    padded = 256**2 * 3 + 1280**2 + 1536**2 + 2048**2
+    assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * padded
+    lib.b2p_ragged_plan_destroy(h)
+    for bad in ({"pad_step": 96}, {"pad_step_large": 32}, {"large_path": _lib.PATHS["blocked"]}, {"dense_min_n": -1}):
+        st, h = _plan_ex(orders, _lib.MODE_BF16X3, **bad)
+        assert st == _lib.B2P_ERR_INVALID_ARG and not h.value, bad
+    # null options = defaults
+    offs = (ctypes.c_int64 * 2)(*inputs.pack_offsets([300, 40])[:-1])
+    ns = (ctypes.c_int32 * 2)(300, 40)
+    h = ctypes.c_void_p()
+    assert lib.b2p_ragged_plan_create_ex(offs, ns, 2, _lib.MODE_BF16X3, None, ctypes.byref(h)) == _lib.B2P_OK
+    assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * 320**2
+    lib.b2p_ragged_plan_destroy(h)
