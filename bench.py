@@ -14,6 +14,8 @@ the plain FP32 form and cuSOLVER on the same GPU are reported beside it.
 Other workloads (profiling and extra lines, not the headline):
   small   4096 x 32 (HBM-bound; 8 rotating input sets, 256 MiB > L2)
   large   1 x 8192 (GG^T/n + 0.1 I)
+  ragged  3000 matrices, n log-uniform in [16, 2048], packed (one ragged plan
+          replayed from a CUDA graph; --autotune picks the plan options)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--mode auto|fp32|bf16x3|tf32]
     python bench.py --impl reference     # the reference's CPU route, timed on host cores
@@ -58,6 +60,18 @@ WORKLOADS = {
         "sets": 8,
         "desc": "small batched potrf: 4096x32 FP32, MM^T/n+I",
         "metric": "batched potrf us per step (4096x32)",
+    },
+    "ragged": {
+        "ragged": True,
+        "count": 3000,
+        "orders_seed": 4,
+        "seeds": [5],
+        "shapes": [],
+        "gen": "well",
+        "sets": 1,
+        "desc": "ragged potrf: 3000 FP32 SPD matrices, n = round(exp(U[ln16, ln2048])) (seed 4), MM^T/n+I, "
+        "packed with offsets",
+        "metric": "ragged potrf us per step (3000 matrices, n log-uniform in [16, 2048])",
     },
     "large": {
         "shapes": [(1, 8192)],
@@ -190,6 +204,8 @@ def run_reference(args) -> int:
     wl = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
+    if wl.get("ragged"):
+        return _run_reference_ragged(args, wl, ws, threads)
     sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
     data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for _ in range(args.warmup):
@@ -231,6 +247,64 @@ def run_reference(args) -> int:
     return 0
 
 
+def _ragged_cpu_sample(orders, offsets, host_buf=None):
+    """Every 50th matrix of the draw (from the packed host buffer when given,
+    else freshly generated with the same distribution)."""
+    from gpumode_cholesky_b200 import inputs
+
+    idx = list(range(0, len(orders), 50))
+    if host_buf is not None:
+        mats = [host_buf[offsets[i] : offsets[i] + orders[i] ** 2].view(1, orders[i], orders[i]) for i in idx]
+    else:
+        mats = [inputs.well_conditioned(1, orders[i], seed=1000 + i, device="cpu") for i in idx]
+    scale = sum(n**3 for n in orders) / sum(orders[i] ** 3 for i in idx)
+    return mats, scale
+
+
+def _run_reference_ragged(args, wl, ws: int, threads: int) -> int:
+    """Reference CPU route per matrix on every 50th matrix of the draw, scaled by sum n^3."""
+    import oracle
+    from gpumode_cholesky_b200 import inputs
+
+    orders = inputs.ragged_orders(wl["count"], seed=wl["orders_seed"])
+    mats, scale = _ragged_cpu_sample(orders, None)
+    for m in mats:
+        oracle.ref_kernel_cpu(m)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for m in mats:
+            oracle.ref_kernel_cpu(m)
+    dt = (time.perf_counter() - t0) / args.steps
+    us = dt * 1e6 * scale
+    line = {
+        "impl": "reference",
+        "metric": wl["metric"],
+        "value": round(us, 1),
+        "unit": "us",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(us / 1000.0, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": wl["desc"], "l2": "inputs larger than L2"},
+        "cpu_baseline": {
+            "value": round(us, 1),
+            "unit": "us",
+            "cores": threads,
+            "kind": "reference",
+            "sample": f"torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) per matrix on every 50th "
+            f"order of the draw ({len(mats)} matrices), scaled by sum n^3 x{scale:.1f}",
+        },
+        "e2e": {"value": round(us, 1), "unit": "us", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 # ---------------------------------------------------------------------------
 def _timed(fn, k: int) -> float:
     """Mean ms per call of k calls, CUDA events on the current stream."""
@@ -244,7 +318,188 @@ def _timed(fn, k: int) -> float:
     return e0.elapsed_time(e1) / k
 
 
+def run_ours_ragged(args, wl) -> int:
+    """The ragged workload: one plan over the whole packed draw, graph-replayed."""
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from gpumode_cholesky_b200 import _lib, build, inputs
+    from gpumode_cholesky_b200.potrf import resolve_mode
+    from gpumode_cholesky_b200.ragged import RaggedPlan, autotune
+
+    if not build.LIB_PATH.exists():
+        build.build()
+    _lib.load()
+    orders = inputs.ragged_orders(wl["count"], seed=wl["orders_seed"])
+    buf, offs = inputs.ragged_batch(orders, seed=wl["seeds"][0] + 7919 * rank, device=dev)
+    offsets = offs[:-1]
+    code = resolve_mode(args.mode, max(orders))
+    tuned = None
+    if args.autotune:
+        plan, res = autotune(buf, orders, offsets, mode=code)
+        tuned = sorted(({"options": o, "us": round(t, 1)} for o, t in res), key=lambda r: r["us"])
+    else:
+        plan = RaggedPlan(orders, offsets, mode=code, device=dev)
+    out = torch.empty_like(buf)
+    graph = plan.capture(buf, out)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    clk = _clock_sampler_start(local)
+    time.sleep(0.3)
+    for _ in range(args.warmup):
+        graph.replay()
+    barrier()
+    torch.cuda.synchronize()
+    t_start = time.time()
+    ms = _timed(graph.replay, args.steps)
+    torch.cuda.synchronize()
+    t_end = time.time()
+    barrier()
+    clocks = _clock_sampler_stop(clk, t_start, t_end)
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    with _lib.LaunchTrace() as tr:
+        plan.factor(buf, out)
+    totals = tr.totals()
+    launches_per_step = sum(c for c, _ in totals.values())
+    # Roofline of the tensor-core kernels of the padded dense groups (the
+    # fused, warp-specialized and split kernels together factor every matrix
+    # with n > 128): algorithmic n^3/3 flops of those matrices over their
+    # time.  The groups run on several streams, so the traced (serialised)
+    # per-kernel sums overstate that time; the dense kernels' time is the
+    # timed step minus the other launches, which run alone on the stream.
+    dense_names = [k for k in totals if k.startswith(("potrf_fused", "split_"))]
+    other_ms = sum(t for k, (_, t) in totals.items() if k not in dense_names)
+    big_flops = sum(n**3 / 3.0 for n in orders if n > 128)
+    peaks = _measured_peaks()
+    roof = None
+    if dense_names:
+        t_dense = max(ms - other_ms, 1e-6)
+        achieved = big_flops / (t_dense / 1000.0) / 1e12
+        roof = {
+            "kernel": "+".join(sorted(dense_names)),
+            "bound": "tensor",
+            "achieved": round(achieved, 3),
+            "peak": peaks["bf16_tflops"],
+            "unit": "TFLOP/s",
+            "frac": round(achieved / peaks["bf16_tflops"], 5),
+            "peak_src": "dense BF16 cuBLAS " + peaks["src"] + " (algorithmic n^3/3 flops of the n > 128 matrices)",
+            "algorithmic_flops": big_flops,
+            "traffic": None,
+            "share_of_step": round(t_dense / ms, 4),
+            "ms": round(t_dense, 4),
+        }
+
+    extra = {}
+    e2e = None
+    cpu = None
+    if not args.quick:
+        worst = 0.0
+        for n, o in zip(orders, offsets):
+            if n > 1000 or n % 97 == 0:
+                ld = out[o : o + n * n].view(n, n).double()
+                ad = buf[o : o + n * n].view(n, n).double()
+                worst = max(worst, (torch.linalg.norm(ld @ ld.T - ad) / torch.linalg.norm(ad)).item())
+        extra["rel_residual_fro_max"] = worst
+        extra["sum_n3_over_3"] = sum(n**3 / 3.0 for n in orders)
+        host_in = buf.cpu().pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        dev_in = torch.empty_like(buf)
+
+        def e2e_step():
+            dev_in.copy_(host_in, non_blocking=True)
+            plan.factor(dev_in, out)
+            host_out.copy_(out, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = _timed(e2e_step, 2)
+        nbytes = host_in.numel() * 4
+        e2e = {"value": round(e2e_ms * 1000, 1), "unit": "us", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+        if rank == 0 and ws == 1 and not args.no_cpu:
+            import oracle
+
+            threads = os.cpu_count() or 1
+            torch.set_num_threads(threads)
+            mats, scale = _ragged_cpu_sample(orders, offsets, host_in)
+            for m in mats:
+                oracle.ref_kernel_cpu(m)
+            t0 = time.perf_counter()
+            for m in mats:
+                oracle.ref_kernel_cpu(m)
+            dt = time.perf_counter() - t0
+            cpu = {
+                "value": round(dt * 1e6 * scale, 1),
+                "unit": "us",
+                "cores": threads,
+                "kind": "reference",
+                "sample": f"torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) per matrix on every 50th "
+                f"matrix ({len(mats)}), scaled by sum n^3 x{scale:.1f}",
+            }
+
+    if rank == 0:
+        line = {
+            "metric": wl["metric"],
+            "value": round(ms * 1000, 1),
+            "unit": "us",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": wl["desc"],
+                "mode": args.mode,
+                "plan_options": {k: getattr(plan.options, k) for k, _ in plan.options._fields_},
+                "l2": "inputs larger than L2 (5.2 GB packed); no flush",
+                "timing": "CUDA-graph replay of the whole ragged plan, CUDA events, max over ranks",
+                "parallelism": f"weak scaling, {ws} rank(s) each a full draw",
+            },
+            **extra,
+            "autotune": tuned,
+            "matrices_per_s": round(ws * len(orders) / (ms / 1000.0), 1),
+            "gflops_per_s": round(ws * sum(n**3 / 3.0 for n in orders) / (ms / 1000.0) / 1e9, 1),
+            "roofline": roof,
+            "kernels_one_step": {k: {"launches": c, "ms": round(t, 4)} for k, (c, t) in sorted(totals.items())},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    del graph
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args) -> int:
+    wl0 = WORKLOADS[args.workload]
+    if wl0.get("ragged"):
+        return run_ours_ragged(args, wl0)
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -519,6 +774,7 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="timed region and roofline only (for profiling)")
     ap.add_argument("--scale", type=float, default=1.0, help="batch scale (small profiling cases); 1 = the workload")
+    ap.add_argument("--autotune", action="store_true", help="ragged workload: time the plan options first")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -38,6 +38,7 @@ class RaggedOptions(ctypes.Structure):
         ("pad_step", ctypes.c_int32),
         ("pad_step_large", ctypes.c_int32),
         ("large_path", ctypes.c_int32),
+        ("streams", ctypes.c_int32),
     ]
 
 # Every symbol the header declares, with (restype, argtypes).

@@ -5,14 +5,17 @@
 //   n <= 32     one persistent warp-per-matrix launch (potrf_warp32_kernel)
 //   n <= 128    one persistent CTA-per-matrix launch  (potrf_cta128_kernel)
 //   n >  128, tensor modes, n >= dense_min_n: padded dense groups.  Each
-//               matrix is padded to p = n rounded up to 64 (identity in the
-//               padding: the Schur complement of the padded rows stays the
-//               identity, so L and info of the first n rows are those of the
-//               unpadded matrix); matrices of equal p form one dense batch
-//               that runs on the n > 128 dispatcher's path for (count, p)
-//               (potrf_fused / potrf_fused_ws / potrf_split).  One gather
-//               launch copies every such matrix into the padded buffer and
-//               one scatter launch copies the factors (and info) back.
+//               matrix is padded to p = n rounded up to the pad step (128 by
+//               default; identity in the padding: the Schur complement of
+//               the padded rows stays the identity, so L and info of the
+//               first n rows are those of the unpadded matrix); matrices of
+//               equal p form one dense batch that runs on the n > 128
+//               dispatcher's path for (count, p) (potrf_fused /
+//               potrf_fused_ws), above 1024 on potrf_fused_ws (or
+//               potrf_split), the groups spread over several streams.  One
+//               gather launch copies every such matrix into the padded
+//               buffer and one scatter launch copies the factors (and info)
+//               back.
 //   n >  128 otherwise (FP32, or below dense_min_n): the blocked
 //               right-looking schedule over all of them at once: matrices
 //               sorted by n (descending), so the matrices still active at
@@ -31,6 +34,7 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <vector>
@@ -41,7 +45,13 @@ namespace b2p {
 
 namespace {
 
-constexpr int kPadStep = 64;        // padded orders are multiples of this
+// Defaults of the plan options, measured on B200 with the 3000-matrix
+// log-uniform [16, 2048] draw (BF16x3): pad steps 128/128, warp-specialized
+// groups above 1024, 4 streams: 16.7 ms; the same on one stream 23.2 ms;
+// pad steps 64/64 on the split path, one stream: 30.4 ms.
+constexpr int kPadStep = 128;       // padded orders are multiples of this
+constexpr int kPadStepLarge = 128;  // ... above 1024
+constexpr int kDefaultStreams = 4;
 constexpr int kTrailTcMinN = 256;   // blocked schedule: tcgen05 trailing update from this order
 constexpr int kDefaultDenseMinN = 129;
 constexpr int kCopyRows = 32;       // rows per gather / scatter item
@@ -120,10 +130,46 @@ size_t align1k(size_t x) { return (x + 1023) & ~(size_t)1023; }
 struct DenseGroup {
   int p = 0;
   int path = 0;
+  int stream = 0;       // 0: the caller's stream, else a library stream
   int64_t first = 0;    // first entry
   int64_t count = 0;
   int64_t elem = 0;     // element offset of the group in the padded buffers
+  size_t ws_off = 0;    // dense-path workspace (offset from the dense area)
+  size_t ws_bytes = 0;
 };
+
+constexpr int kRaggedMaxStreams = 8;
+
+namespace {
+// Per device: the library streams dense groups run on, with the events that
+// fork them from and join them to the caller's stream.
+struct GroupStreams {
+  cudaStream_t st[kRaggedMaxStreams] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join[kRaggedMaxStreams] = {};
+};
+constexpr int kGroupStreamDevices = 64;
+GroupStreams g_gs[kGroupStreamDevices];
+std::mutex g_gs_mu;
+
+int group_streams(GroupStreams** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kGroupStreamDevices)
+    return set_error(B2P_ERR_CUDA, "no usable current device");
+  std::lock_guard<std::mutex> lock(g_gs_mu);
+  GroupStreams& gs = g_gs[dev];
+  if (gs.fork == nullptr) {
+    cudaError_t e = cudaEventCreateWithFlags(&gs.fork, cudaEventDisableTiming);
+    for (int i = 1; i < kRaggedMaxStreams && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&gs.st[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&gs.join[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "ragged streams: %s", cudaGetErrorString(e));
+  }
+  *out = &gs;
+  return B2P_OK;
+}
+}  // namespace
 
 struct RaggedPlanImpl {
   int mode = 0;
@@ -131,6 +177,7 @@ struct RaggedPlanImpl {
   int64_t count = 0;
   int64_t n_small = 0, n_mid = 0, n_big = 0, n_dense = 0, n_items = 0;
   int max_n = 0;
+  int nstreams = 1;
   std::vector<RaggedStep> steps;       // SIMT trail items
   std::vector<RaggedStep> steps_tc;    // tcgen05 trail items (tensor modes)
   std::vector<DenseGroup> groups;
@@ -167,10 +214,12 @@ int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host
   if (options != nullptr) opt = *options;
   auto step_ok = [](int v) { return v == 0 || v == 64 || v == 128 || v == 256; };
   if (opt.dense_min_n < 0 || !step_ok(opt.pad_step) || !step_ok(opt.pad_step_large) ||
-      (opt.large_path != B2P_PATH_AUTO && opt.large_path != B2P_PATH_SPLIT && opt.large_path != B2P_PATH_FUSED_WS))
-    return set_error(B2P_ERR_INVALID_ARG, "bad ragged options (pad steps 64/128/256; large path auto/split/fused_ws)");
+      (opt.large_path != B2P_PATH_AUTO && opt.large_path != B2P_PATH_SPLIT && opt.large_path != B2P_PATH_FUSED_WS) ||
+      opt.streams < 0 || opt.streams > kRaggedMaxStreams)
+    return set_error(B2P_ERR_INVALID_ARG,
+                     "bad ragged options (pad steps 64/128/256; large path auto/split/fused_ws; streams 0..8)");
   const int step_small = opt.pad_step ? opt.pad_step : kPadStep;
-  const int step_large = opt.pad_step_large ? opt.pad_step_large : kPadStep;
+  const int step_large = opt.pad_step_large ? opt.pad_step_large : kPadStepLarge;
   if (count < 0 || (count > 0 && (offsets_host == nullptr || n_host == nullptr)))
     return set_error(B2P_ERR_INVALID_ARG, "bad ragged list");
   const int m = mode & B2P_MODE_MASK;
@@ -265,7 +314,7 @@ int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host
     g.count = (int64_t)kv.second.size();
     g.elem = elem;
     g.path = choose_path(g.count, g.p, mode);
-    if (g.p > 1024 && opt.large_path == B2P_PATH_FUSED_WS && fused_ws_fits(g.count, g.p, mode))
+    if (g.p > 1024 && opt.large_path != B2P_PATH_SPLIT && fused_ws_fits(g.count, g.p, mode))
       g.path = B2P_PATH_FUSED_WS;
     const bool ok = g.path == B2P_PATH_FUSED_WS ? fused_ws_fits(g.count, g.p, mode)
                                                  : path_supported(g.path, g.count, g.p, mode);
@@ -286,8 +335,36 @@ int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host
       dents.push_back(e);
       elem += (int64_t)g.p * g.p;
     }
-    p.ws_dense_bytes = std::max(p.ws_dense_bytes, path_workspace_bytes(g.path, g.count, g.p, mode));
+    g.ws_bytes = path_workspace_bytes(g.path, g.count, g.p, mode);
     p.groups.push_back(g);
+  }
+  // Streams: the largest groups first, each onto the least loaded stream
+  // (work ~ count p^3); split-path groups stay on the caller's stream, since
+  // their look-ahead shares one side stream per device.
+  p.nstreams = std::max(1, std::min<int>(opt.streams ? opt.streams : kDefaultStreams, (int)p.groups.size()));
+  {
+    std::vector<double> load(p.nstreams, 0.0);
+    std::vector<size_t> order(p.groups.size());
+    std::iota(order.begin(), order.end(), 0);
+    auto work = [&](const DenseGroup& g) { return (double)g.count * g.p * g.p * g.p; };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t x, size_t y) { return work(p.groups[x]) > work(p.groups[y]); });
+    for (size_t gi : order) {
+      DenseGroup& g = p.groups[gi];
+      int best = 0;
+      if (g.path != B2P_PATH_SPLIT)
+        for (int i = 1; i < p.nstreams; ++i)
+          if (load[i] < load[best]) best = i;
+      g.stream = best;
+      load[best] += work(g);
+    }
+    std::vector<size_t> need(p.nstreams, 0), off(p.nstreams, 0);
+    for (const DenseGroup& g : p.groups) need[g.stream] = std::max(need[g.stream], g.ws_bytes);
+    for (int i = 0; i < p.nstreams; ++i) {
+      off[i] = p.ws_dense_bytes;
+      p.ws_dense_bytes = align1k(p.ws_dense_bytes + need[i]);
+    }
+    for (DenseGroup& g : p.groups) g.ws_off = off[g.stream];
   }
   p.n_items = (int64_t)ditems.size();
   // Workspace: blocked diagonal tiles, padded A and L, group info, dense path workspace.
@@ -397,10 +474,25 @@ int b2p_potrf_ragged(const b2p_ragged_plan* plan, const void* tables, const floa
       ragged_gather_kernel<<<grid, kCopyThreads, 0, s>>>(a, ap, ents, ditems, p.n_items);
       if (int st = check_launch("ragged_gather_kernel")) return st;
     }
+    GroupStreams* gs = nullptr;
+    auto check = [](cudaError_t e, const char* what) -> int {
+      return e == cudaSuccess ? B2P_OK : set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    };
+    if (p.nstreams > 1) {
+      if (int st = group_streams(&gs)) return st;
+      if (int st = check(cudaEventRecord(gs->fork, s), "cudaEventRecord")) return st;
+      for (int i = 1; i < p.nstreams; ++i)
+        if (int st = check(cudaStreamWaitEvent(gs->st[i], gs->fork, 0), "cudaStreamWaitEvent")) return st;
+    }
     for (const DenseGroup& g : p.groups) {
-      if (int st = potrf_path(ap + g.elem, lp + g.elem, g.count, g.p, p.mode, g.path, wsb + p.ws_dense,
-                              p.ws_dense_bytes, info ? ginfo + g.first : nullptr, s))
+      cudaStream_t gst = g.stream == 0 ? s : gs->st[g.stream];
+      if (int st = potrf_path(ap + g.elem, lp + g.elem, g.count, g.p, p.mode, g.path, wsb + p.ws_dense + g.ws_off,
+                              g.ws_bytes, info ? ginfo + g.first : nullptr, gst))
         return st;
+    }
+    for (int i = 1; i < p.nstreams; ++i) {
+      if (int st = check(cudaEventRecord(gs->join[i], gs->st[i]), "cudaEventRecord")) return st;
+      if (int st = check(cudaStreamWaitEvent(s, gs->join[i], 0), "cudaStreamWaitEvent")) return st;
     }
     {
       TraceScope ts(kKRaggedScatter, s);

@@ -47,9 +47,10 @@ class RaggedPlan:
     are factored as identity-padded dense batches, one per padded order
     (multiple of ``pad_step``, or ``pad_step_large`` above 1024: 64, 128 or
     256); smaller ones take the blocked ragged schedule.  ``large_path``
-    picks the algorithm of the groups above 1024 ("split" or "fused_ws").
-    Zero / "auto" take the library defaults (every n > 128 padded to a
-    multiple of 64; split above 1024).
+    picks the algorithm of the groups above 1024 ("split" or "fused_ws");
+    ``streams`` runs the groups on that many streams at once.  Zero / "auto"
+    take the library defaults (every n > 128 padded to a multiple of 128,
+    warp-specialized groups above 1024, four streams).
     """
 
     def __init__(
@@ -62,6 +63,7 @@ class RaggedPlan:
         pad_step: int = 0,
         pad_step_large: int = 0,
         large_path: str = "auto",
+        streams: int = 0,
     ):
         self.orders = [int(n) for n in orders]
         self.offsets = [int(o) for o in (offsets if offsets is not None else pack_offsets(self.orders)[:-1])]
@@ -77,7 +79,9 @@ class RaggedPlan:
         handle = ctypes.c_void_p()
         if large_path not in ("auto", "split", "fused_ws"):
             raise ValueError(f"large_path must be auto, split or fused_ws, not {large_path!r}")
-        self.options = _lib.RaggedOptions(int(tc_min_n), int(pad_step), int(pad_step_large), _lib.PATHS[large_path])
+        self.options = _lib.RaggedOptions(
+            int(tc_min_n), int(pad_step), int(pad_step_large), _lib.PATHS[large_path], int(streams)
+        )
         _lib.check(
             lib.b2p_ragged_plan_create_ex(
                 offs, ns, self.count, self.mode, ctypes.byref(self.options), ctypes.byref(handle)
@@ -138,6 +142,66 @@ class RaggedPlan:
         with torch.cuda.graph(g):
             self.factor(a_static, out_static)
         return g
+
+
+#: Candidate plan options for :func:`autotune`: padded-order step for orders
+#: <= 1024 and above, path of the groups above 1024, and concurrent streams.
+AUTOTUNE_GRID: tuple[dict, ...] = tuple(
+    {"pad_step": ps, "pad_step_large": pl, "large_path": lp, "streams": st}
+    for ps in (64, 128)
+    for pl in (128, 256)
+    for lp in ("fused_ws", "split")
+    for st in (1, 4)
+)
+
+
+def autotune(
+    a: torch.Tensor,
+    orders: Sequence[int],
+    offsets: Sequence[int] | None = None,
+    mode: str | int | None = "bf16x3",
+    candidates: Sequence[dict] | None = None,
+    reps: int = 2,
+) -> tuple[RaggedPlan, list[tuple[dict, float]]]:
+    """Pick the fastest plan options for this list of orders on this GPU.
+
+    Every candidate (default :data:`AUTOTUNE_GRID`: the padded-order steps per
+    size bucket, the path of the large groups, the stream count) is built,
+    captured in a CUDA graph over the packed buffer ``a`` and timed with CUDA
+    events (one warm-up replay, then ``reps``).  Returns the fastest plan and
+    the (options, microseconds) of every candidate.  The candidates differ
+    only in grouping and scheduling; all factor every matrix in the same
+    precision mode.
+    """
+    cands = list(candidates if candidates is not None else AUTOTUNE_GRID)
+    if not cands:
+        raise ValueError("no candidate options")
+    out = torch.empty_like(a)
+    results: list[tuple[dict, float]] = []
+    best_us, best = float("inf"), None
+    for opt in cands:
+        plan = RaggedPlan(orders, offsets, mode=mode, device=a.device, **opt)
+        g = plan.capture(a, out)
+        g.replay()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(reps):
+            g.replay()
+        end.record()
+        end.synchronize()
+        us = start.elapsed_time(end) * 1000.0 / reps
+        results.append((dict(opt), us))
+        del g
+        if us < best_us:
+            if best is not None:
+                best.close()
+            best_us, best = us, plan
+        else:
+            plan.close()
+        del plan
+        torch.cuda.empty_cache()
+    assert best is not None
+    return best, results
 
 
 def cholesky_ragged(

@@ -138,10 +138,10 @@ B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, i
  *                            every launch.  tc_min_n (tensor modes; 0 =
  *                            default 129): matrices of at least this order
  *                            (and > 128) are copied into identity-padded
- *                            dense batches (order rounded up to 64, one
- *                            batch per padded order) and factored on the
- *                            dense tensor-core paths; smaller ones take the
- *                            blocked ragged schedule;
+ *                            dense batches (order rounded up to the pad
+ *                            step, one batch per padded order) and factored
+ *                            on the dense tensor-core paths; smaller ones
+ *                            take the blocked ragged schedule;
  *   b2p_ragged_plan_upload   copies the plan's tables (table_bytes, 16-byte
  *                            aligned device buffer) to the device; blocking;
  *   b2p_potrf_ragged         enqueues the factorization; reads only device
@@ -162,19 +162,25 @@ B2P_API int b2p_ragged_plan_create(const int64_t* offsets_host, const int32_t* n
  * b2p_ragged_plan_create_ex with dense_min_n = tc_min_n and the rest zero.
  *   dense_min_n     as tc_min_n above (default 129)
  *   pad_step        padded-order granularity for orders <= 1024: 64, 128 or
- *                   256 (default 64); coarser steps make fewer, larger groups
- *                   at the cost of padding work
- *   pad_step_large  the same for orders > 1024 (default 64)
+ *                   256 (default 128); coarser steps make fewer, larger
+ *                   groups at the cost of padding work
+ *   pad_step_large  the same for orders > 1024 (default 128)
  *   large_path      path of the groups with padded order > 1024:
- *                   B2P_PATH_AUTO (= SPLIT), B2P_PATH_SPLIT or
+ *                   B2P_PATH_AUTO (= FUSED_WS up to 8192, SPLIT above),
  *                   B2P_PATH_FUSED_WS (clusters of CTAs per matrix, one
- *                   launch per group; orders up to 8192)
+ *                   launch per group) or B2P_PATH_SPLIT
+ *   streams         groups run on this many streams at once (1..8, default
+ *                   4): the caller's stream and library-owned ones, forked
+ *                   from and joined back into the caller's stream with
+ *                   events (capturable); groups on the split path stay on
+ *                   the caller's stream
  */
 typedef struct b2p_ragged_options {
   int32_t dense_min_n;
   int32_t pad_step;
   int32_t pad_step_large;
   int32_t large_path;
+  int32_t streams;
 } b2p_ragged_options;
 B2P_API int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host, int64_t count,
                                       int mode, const b2p_ragged_options* options, b2p_ragged_plan** plan);

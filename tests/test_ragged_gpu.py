@@ -103,7 +103,9 @@ def test_ragged_dense_groups_bitwise_equal_padded_dense():
     orders = [200, 150, 256, 300, 1000, 1100, 1090, 40]
     mats = [inputs.generate_input(1, n, 2, 17 + n, "dense", device="cpu")[0] for n in orders]
     buf, orders, offs = pack(mats, device="cuda")
-    plan = RaggedPlan(orders, offs, mode="bf16x3")
+    # Pad steps of 64 and the split path above 1024: the groups are exactly
+    # the batches the dense dispatcher would see.
+    plan = RaggedPlan(orders, offs, mode="bf16x3", pad_step=64, pad_step_large=64, large_path="split")
     plan.workspace.fill_(0xFF)
     info = torch.full((len(orders),), -5, dtype=torch.int32, device="cuda")
     out = plan.factor(buf, info=info)
@@ -121,6 +123,29 @@ def test_ragged_dense_groups_bitwise_equal_padded_dense():
             n = orders[i]
             assert torch.equal(ls[i], dense[j, :n, :n]), (n, p)
             assert torch.equal(dense[j, n:, n:], torch.eye(p - n, device="cuda")), (n, p)
+
+
+def test_ragged_options_same_factors():
+    """Stream count and the large-group path change the schedule, not the
+    arithmetic of a group: factors are bitwise those of the one-stream plan
+    with the same pad steps; graph capture works with several streams."""
+    orders = [150, 150, 200, 300, 520, 640, 1000, 1100, 1300, 60, 20]
+    mats = [inputs.well_conditioned(1, n, seed=3 * n, device="cpu")[0] for n in orders]
+    buf, orders, offs = pack(mats, device="cuda")
+    base = RaggedPlan(orders, offs, mode="bf16x3", large_path="fused_ws", streams=1).factor(buf)
+    plan = RaggedPlan(orders, offs, mode="bf16x3", large_path="fused_ws", streams=4)
+    out = torch.zeros_like(buf)
+    g = plan.capture(buf, out)
+    out.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out, base)
+    split = RaggedPlan(
+        orders, offs, mode="bf16x3", pad_step=128, pad_step_large=256, large_path="split", streams=3
+    ).factor(buf)
+    for m, l in zip(mats, unpack(split, orders, offs)):
+        ld, ad = l.double(), m.cuda().double()
+        assert (torch.linalg.norm(ld @ ld.T - ad) / torch.linalg.norm(ad)).item() <= 1e-5
 
 
 @pytest.mark.parametrize("mode", ["bf16x3", "tf32", "fp32"])

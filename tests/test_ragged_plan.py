@@ -99,7 +99,11 @@ def _plan_ex(orders, mode, **kw):
     offs = (ctypes.c_int64 * max(len(orders), 1))(*offsets)
     ns = (ctypes.c_int32 * max(len(orders), 1))(*orders)
     opt = _lib.RaggedOptions(
-        kw.get("dense_min_n", 0), kw.get("pad_step", 0), kw.get("pad_step_large", 0), kw.get("large_path", 0)
+        kw.get("dense_min_n", 0),
+        kw.get("pad_step", 0),
+        kw.get("pad_step_large", 0),
+        kw.get("large_path", 0),
+        kw.get("streams", 0),
     )
     h = ctypes.c_void_p()
     st = lib.b2p_ragged_plan_create_ex(offs, ns, len(orders), mode, ctypes.byref(opt), ctypes.byref(h))
@@ -114,7 +118,17 @@ def test_plan_options():
     padded = 256**2 * 3 + 1280**2 + 1536**2 + 2048**2
     assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * padded
     lib.b2p_ragged_plan_destroy(h)
-    for bad in ({"pad_step": 96}, {"pad_step_large": 32}, {"large_path": _lib.PATHS["blocked"]}, {"dense_min_n": -1}):
+    st, h = _plan_ex(orders, _lib.MODE_BF16X3, streams=8)
+    assert st == _lib.B2P_OK
+    lib.b2p_ragged_plan_destroy(h)
+    for bad in (
+        {"pad_step": 96},
+        {"pad_step_large": 32},
+        {"large_path": _lib.PATHS["blocked"]},
+        {"dense_min_n": -1},
+        {"streams": 9},
+        {"streams": -1},
+    ):
         st, h = _plan_ex(orders, _lib.MODE_BF16X3, **bad)
         assert st == _lib.B2P_ERR_INVALID_ARG and not h.value, bad
     # null options = defaults
