@@ -13,7 +13,7 @@ the plain FP32 form and cuSOLVER on the same GPU are reported beside it.
 
 Other workloads (profiling and extra lines, not the headline):
   small   4096 x 32 (HBM-bound; 8 rotating input sets, 256 MiB > L2)
-  large   1 x 8192 (GG^T/n + 0.1 I)
+  large   1 x 8192 (GG^T/n + 0.1 I); large16k, large32k: 1 x 16384, 1 x 32768
   ragged  3000 matrices, n log-uniform in [16, 2048], packed (one ragged plan
           replayed from a CUDA graph; --autotune picks the plan options)
 
@@ -80,6 +80,22 @@ WORKLOADS = {
         "sets": 1,
         "desc": "large potrf: 1x8192 FP32, GG^T/n+0.1I",
         "metric": "potrf us per step (1x8192)",
+    },
+    "large16k": {
+        "shapes": [(1, 16384)],
+        "seeds": [416384],
+        "gen": "gram",
+        "sets": 1,
+        "desc": "large potrf: 1x16384 FP32, GG^T/n+0.1I",
+        "metric": "potrf us per step (1x16384)",
+    },
+    "large32k": {
+        "shapes": [(1, 32768)],
+        "seeds": [432768],
+        "gen": "gram",
+        "sets": 1,
+        "desc": "large potrf: 1x32768 FP32, GG^T/n+0.1I",
+        "metric": "potrf us per step (1x32768)",
     },
 }
 

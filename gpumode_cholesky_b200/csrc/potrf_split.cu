@@ -725,6 +725,7 @@ struct SideStream {
   cudaStream_t wide = nullptr;
   cudaEvent_t wide_done[2] = {nullptr, nullptr};
   cudaEvent_t wide_free[2] = {nullptr, nullptr};
+  int step_priority = 0;  // the device's greatest (numerically lowest) priority
 };
 constexpr int kSideDevices = 64;
 SideStream g_side[kSideDevices];
@@ -742,6 +743,9 @@ int side_stream(SideStream** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[0], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.join[1], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ss.wide, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    ss.step_priority = greatest;
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
       e = cudaEventCreateWithFlags(&ss.wide_done[i], cudaEventDisableTiming);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.wide_free[i], cudaEventDisableTiming);
@@ -887,9 +891,22 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     const int G = step_G(k);
     const int grid = (int)step_ctas(k);
     {
+      // The steps carry the critical path: their CTAs go first when the
+      // look-ahead and outer-block kernels compete for SMs (also inside a
+      // CUDA graph, where a kernel node keeps its launch priority).
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)grid, 1, 1);
+      cfg.blockDim = dim3(kSThreads, 1, 1);
+      cfg.dynamicSmemBytes = kSSmemBytes;
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributePriority;
+      attr[0].val.priority = side->step_priority;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
       TraceScope ts(kKSplitStep, s);
-      stp<<<grid, kSThreads, kSSmemBytes, s>>>(a, l, copies, pk, batch, n, k, G, info);
-      if (int st = check_launch("split_step_kernel")) return st;
+      const cudaError_t e = cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info);
+      if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,
     // which are all final once step k, the last of block J - 2, is done.
