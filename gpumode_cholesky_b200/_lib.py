@@ -62,6 +62,9 @@ SIGNATURES = {
     "b2p_noalloc_scratch_bytes": (_c_sz, []),
     "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_ragged_plan_create": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, ctypes.c_int, _c_p]),
+    "b2p_trsv_batched": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p]),
+    "b2p_gp_nll_forward": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_i64, _c_p]),
+    "b2p_gp_nll_backward": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_i64, _c_p]),
     "b2p_ragged_plan_create_ex": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_ragged_plan_destroy": (None, [_c_p]),
     "b2p_ragged_plan_table_bytes": (_c_sz, [_c_p]),

@@ -68,6 +68,10 @@ size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode);
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
                int32_t* info, cudaStream_t s);
 
+// Batched triangular solves with L (trsv.cu): x = L^{-1} b, or L^{-T} b.
+constexpr int kTrsvMaxN = 32768;  // x is held in shared memory (n floats)
+int launch_trsv(const float* l, const float* b, float* x, int64_t batch, int n, bool trans, cudaStream_t s);
+
 // Batched tensor-core GEMM with structure hints (gemm_tc.cu):
 // C = alpha * op1(X) op2(Y) + beta * C per batch item.
 struct GemmArgs {
@@ -111,6 +115,9 @@ enum KernelId {
   kKFusedWs,
   kKRaggedScatter,
   kKSplitWide,
+  kKTrsv,
+  kKGpForward,
+  kKGpLbar,
   kKCount
 };
 
@@ -160,6 +167,9 @@ enum SmemSlot {
   kSlotSplitW0,
   kSlotSplitW1,
   kSlotBwdSmall,
+  kSlotTrsv0,
+  kSlotTrsv1,
+  kSlotGpForward,
   kSlotCount
 };
 

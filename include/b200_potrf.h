@@ -208,6 +208,35 @@ B2P_API int b2p_potrf_backward(const float* l, const float* lbar, float* abar, i
                                void* stream);
 
 /*
+ * Triangular solves with a batch of Cholesky factors (batch x n x n, lower,
+ * row-major FP32, as b2p_potrf_batched writes them): x = L^{-1} b
+ * (trans = 0) or x = L^{-T} b (trans = 1), b and x batch x n (x may alias b).
+ * n <= 32768.  FP32 throughout.  Replaces the reference-side
+ * torch.linalg.solve_triangular a Gaussian-process loss would call on the
+ * factor; the reference itself stops at the factorization.
+ */
+B2P_API int b2p_trsv_batched(const float* l, const float* b, float* x, int64_t batch, int64_t n, int trans,
+                             void* stream);
+
+/*
+ * Gaussian-process negative log-likelihood from the factor L of A = L L^T:
+ *   b2p_gp_nll_forward:  alpha = L^{-1} y and
+ *                        loss[b] = 1/2 alpha^T alpha + sum_i log L_ii
+ *                        (the n/2 log 2pi constant omitted);
+ *   b2p_gp_nll_backward: from alpha and gloss[b] = dOut/dloss[b]:
+ *                        beta = L^{-T} alpha (= A^{-1} y; dOut/dy = gloss beta)
+ *                        and Lbar = gloss (tril(-beta alpha^T) + diag(1/L_ii)),
+ *                        the dOut/dL that b2p_potrf_backward maps to dOut/dA.
+ * y, alpha, beta: batch x n; loss, gloss: batch; lbar: batch x n x n (written
+ * whole, zeros above the diagonal).  n <= 32768.  No counterpart exists in
+ * the reference (forward factorization only).
+ */
+B2P_API int b2p_gp_nll_forward(const float* l, const float* y, float* alpha, float* loss, int64_t batch,
+                               int64_t n, void* stream);
+B2P_API int b2p_gp_nll_backward(const float* l, const float* alpha, const float* gloss, float* beta,
+                                float* lbar, int64_t batch, int64_t n, void* stream);
+
+/*
  * Diagnostic: D[t] = A[t] * B[t]^T for `count` independent pairs of 128x64
  * FP32 tiles (row-major, K contiguous) through the library's tcgen05 staging
  * and MMA path; mode B2P_MODE_TF32 or B2P_MODE_BF16X3; err (device int32,
