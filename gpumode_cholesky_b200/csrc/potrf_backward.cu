@@ -64,32 +64,31 @@ __global__ void sym_kernel(const float* __restrict__ s, float* __restrict__ out,
 }
 
 // ---- n <= 128: one CTA per matrix ------------------------------------------
-constexpr int kBsThreads = 256;
+constexpr int kBsThreads = 512;  // 16 warps: 8 x 4 register tiles over the 128 x 128 products
 constexpr int kBsLd = 132;                      // row stride of the three 128x128 buffers
 constexpr int kBsBuf = 128 * kBsLd;             // floats per buffer
 constexpr int kBsWork = 4 * 32 * 33;            // smem_trtri's work area
 constexpr size_t kBsSmemBytes = sizeof(float) * (size_t)(3 * kBsBuf + kBsWork + 128 + 4);
 
-// acc[r][c] = sum_{k in [k0, k1)} X[k][8ti + r] * Y[k][8tj + c] (X, Y row-major
+// acc[r][c] = sum_{k in [k0, k1)} X[k][8ti + r] * Y[k][4tj + c] (X, Y row-major
 // in shared memory, row stride kBsLd): the X^T Y tile of this thread.
 __device__ __forceinline__ void bs_tile(const float* X, const float* Y, int ti, int tj, int k0, int k1,
-                                        float (&acc)[8][8]) {
+                                        float (&acc)[8][4]) {
 #pragma unroll
   for (int r = 0; r < 8; ++r)
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
 #pragma unroll 2
   for (int k = k0; k < k1; ++k) {
     const float4 x0 = *reinterpret_cast<const float4*>(X + k * kBsLd + 8 * ti);
     const float4 x1 = *reinterpret_cast<const float4*>(X + k * kBsLd + 8 * ti + 4);
-    const float4 y0 = *reinterpret_cast<const float4*>(Y + k * kBsLd + 8 * tj);
-    const float4 y1 = *reinterpret_cast<const float4*>(Y + k * kBsLd + 8 * tj + 4);
+    const float4 y0 = *reinterpret_cast<const float4*>(Y + k * kBsLd + 4 * tj);
     const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-    const float yv[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+    const float yv[4] = {y0.x, y0.y, y0.z, y0.w};
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
+      for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
   }
 }
 
@@ -104,8 +103,8 @@ __global__ void __launch_bounds__(kBsThreads, 1)
   TileScratch sc{};
   sc.invd = work + kBsWork;
   const int tid = threadIdx.x;
-  const int ti = tid >> 4, tj = tid & 15;
-  float acc[8][8];
+  const int ti = tid >> 5, tj = tid & 31;  // rows 8ti.., columns 4tj..
+  float acc[8][4];
   for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
     const float* L = l + (size_t)b * n * n;
     const float* G = lbar + (size_t)b * n * n;
@@ -118,16 +117,18 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     }
     __syncthreads();
     if (tid < 128) sc.invd[tid] = 1.0f / bA[tid * kBsLd + tid];
-    // P = Phi(L^T Lbar) (lower tiles; k >= max(i, j)), kept in registers.
-    const bool lower = tj <= ti;
-    if (lower) bs_tile(bA, bB, ti, tj, 8 * ti, 128, acc);
+    // P = Phi(L^T Lbar) (tiles reaching the lower triangle; k >= max(i, j)),
+    // kept in registers.
+    const bool lower = 4 * tj <= 8 * ti + 7;
+    const int kmax = 8 * ti > 4 * tj ? 8 * ti : 4 * tj;  // smallest max(i, j) of the tile
+    if (lower) bs_tile(bA, bB, ti, tj, kmax, 128, acc);
     __syncthreads();
     // P^T into bB.
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int i = 8 * ti + r, j = 8 * tj + c;
+      for (int c = 0; c < 4; ++c) {
+        const int i = 8 * ti + r, j = 4 * tj + c;
         const float v = !lower || j > i ? 0.0f : (j == i ? 0.5f * acc[r][c] : acc[r][c]);
         bB[j * kBsLd + i] = v;
       }
@@ -135,22 +136,22 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     smem_trtri<kBsThreads>(bA, 128, kBsLd, bC, kBsLd, sc, work);
     __syncthreads();
     // Z = P U: Z[i][j] = sum_k P^T[k][i] U[k][j], k in [j, i] (lower tiles).
-    if (lower) bs_tile(bB, bC, ti, tj, 8 * tj, 8 * ti + 8, acc);
+    if (lower) bs_tile(bB, bC, ti, tj, 4 * tj, 8 * ti + 8, acc);
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const int i = 8 * ti + r, j = 8 * tj + c;
+      for (int c = 0; c < 4; ++c) {
+        const int i = 8 * ti + r, j = 4 * tj + c;
         bB[i * kBsLd + j] = (lower && j <= i) ? acc[r][c] : 0.0f;
       }
     __syncthreads();
     // S = U^T Z: S[i][j] = sum_k U[k][i] Z[k][j], k >= max(i, j); into bA.
-    bs_tile(bC, bB, ti, tj, 8 * (ti > tj ? ti : tj), 128, acc);
+    bs_tile(bC, bB, ti, tj, kmax, 128, acc);
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-      for (int c = 0; c < 8; ++c) bA[(8 * ti + r) * kBsLd + 8 * tj + c] = acc[r][c];
+      for (int c = 0; c < 4; ++c) bA[(8 * ti + r) * kBsLd + 4 * tj + c] = acc[r][c];
     __syncthreads();
     float* Ab = abar + (size_t)b * n * n;
     for (int e = tid; e < n * n; e += kBsThreads) {
