@@ -16,6 +16,8 @@ Other workloads (profiling and extra lines, not the headline):
   large   1 x 8192 (GG^T/n + 0.1 I); large16k, large32k: 1 x 16384, 1 x 32768
   ragged  3000 matrices, n log-uniform in [16, 2048], packed (one ragged plan
           replayed from a CUDA graph; --autotune picks the plan options)
+  gp      Gaussian-process loss, forward and backward through autograd
+          (eager calls), 256 x 128 + 8 x 2048 RBF kernels
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--mode auto|fp32|bf16x3|tf32]
     python bench.py --impl reference     # the reference's CPU route, timed on host cores
@@ -72,6 +74,16 @@ WORKLOADS = {
         "desc": "ragged potrf: 3000 FP32 SPD matrices, n = round(exp(U[ln16, ln2048])) (seed 4), MM^T/n+I, "
         "packed with offsets",
         "metric": "ragged potrf us per step (3000 matrices, n log-uniform in [16, 2048])",
+    },
+    "gp": {
+        "gp": True,
+        "shapes": [(256, 128), (8, 2048)],
+        "seeds": [5128, 52048],
+        "gen": "rbf",
+        "sets": 1,
+        "desc": "GP log-likelihood forward+backward: 256x128 + 8x2048 FP32 RBF kernels over U[0,1]^3 points, "
+        "lengthscale U[0.2,0.5], variance 1, jitter 1e-4 I, y ~ N(0,1)",
+        "metric": "gp nll fwd+bwd us per step (256x128 + 8x2048)",
     },
     "large": {
         "shapes": [(1, 8192)],
@@ -222,6 +234,9 @@ def run_reference(args) -> int:
     torch.set_num_threads(threads)
     if wl.get("ragged"):
         return _run_reference_ragged(args, wl, ws, threads)
+    if wl.get("gp"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no Gaussian-process or backward path (forward factorization only)"}))
+        return 0
     sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
     data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for _ in range(args.warmup):
@@ -512,10 +527,181 @@ def run_ours_ragged(args, wl) -> int:
     return 0
 
 
+def _gp_step(pairs, gp_nll):
+    grads = []
+    for a, y in pairs:
+        aa = a.detach().requires_grad_(True)
+        loss = gp_nll(aa, y).sum()
+        loss.backward()
+        grads.append(aa.grad)
+    return grads
+
+
+def run_ours_gp(args, wl) -> int:
+    """The GP workload: loss and dLoss/dA per step, eager autograd calls."""
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    from gpumode_cholesky_b200 import _lib, build, gp_nll, inputs
+
+    if not build.LIB_PATH.exists():
+        build.build()
+    _lib.load()
+    pairs = [inputs.rbf_kernel_batch(b, n, seed=s + 7919 * rank, device=dev) for (b, n), s in zip(wl["shapes"], wl["seeds"])]
+    clk = _clock_sampler_start(local)
+    time.sleep(0.3)
+    for _ in range(args.warmup):
+        _gp_step(pairs, gp_nll)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = time.time()
+    ms = _timed(lambda: _gp_step(pairs, gp_nll), args.steps)
+    t_end = time.time()
+    clocks = _clock_sampler_stop(clk, t_start, t_end)
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    with _lib.LaunchTrace() as tr:
+        _gp_step(pairs, gp_nll)
+        torch.cuda.synchronize()
+    totals = tr.totals()
+    launches = sum(c for c, _ in totals.values())
+    all_ms = max(sum(t for _, t in totals.values()), 1e-12)
+    dom_name, (dom_count, dom_ms) = max(totals.items(), key=lambda kv: kv[1][1])
+    peaks = _measured_peaks()
+    # Algorithmic flops per step: forward n^3/3, adjoint n^3 (P = Phi(L^T Lbar),
+    # U = L^{-1}, Z = P U, S = U^T Z), both per matrix.
+    fwd_flops = sum(b * n**3 / 3.0 for b, n in wl["shapes"])
+    bwd_flops = sum(b * n**3 for b, n in wl["shapes"])
+    dom_flops = bwd_flops if dom_name.startswith("bwd") else fwd_flops
+    t_dom = ms * dom_ms / all_ms
+    achieved = dom_flops / (t_dom / 1000.0) / 1e12
+    roof = {
+        "kernel": dom_name,
+        "bound": "tensor" if dom_name.startswith("bwd_gemm") else "fp32",
+        "achieved": round(achieved, 3),
+        "peak": peaks["bf16_tflops"],
+        "unit": "TFLOP/s",
+        "frac": round(achieved / peaks["bf16_tflops"], 5),
+        "peak_src": "dense BF16 cuBLAS " + peaks["src"] + " (algorithmic flops of the part this kernel belongs to)",
+        "algorithmic_flops": dom_flops,
+        "traffic": None,
+        "share_of_step": round(dom_ms / all_ms, 4),
+        "launches": dom_count,
+        "ms": round(t_dom, 4),
+    }
+    extra, e2e, cpu = {}, None, None
+    if not args.quick:
+        grads = _gp_step(pairs, gp_nll)
+        errs = {}
+        for (b, n), (a, y), g in zip(wl["shapes"], pairs, grads):
+            from gpumode_cholesky_b200.gp import gp_nll_grad_closed_form
+
+            want = gp_nll_grad_closed_form(a, y)
+            errs[f"{b}x{n}"] = float(torch.linalg.norm((g.double() - want).flatten()) / torch.linalg.norm(want.flatten()))
+        extra["grad_rel_err_vs_fp64"] = errs
+        host = [(a.cpu().pin_memory(), y.cpu().pin_memory()) for a, y in pairs]
+        dev_in = [(torch.empty_like(a), torch.empty_like(y)) for a, y in pairs]
+        outs = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a, _ in host]
+
+        def e2e_step():
+            for (ha, hy), (da, dy), ho in zip(host, dev_in, outs):
+                da.copy_(ha, non_blocking=True)
+                dy.copy_(hy, non_blocking=True)
+                aa = da.detach().requires_grad_(True)
+                gp_nll(aa, dy).sum().backward()
+                ho.copy_(aa.grad, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms = _timed(e2e_step, max(2, args.steps // 2))
+        h2d = sum(a.numel() * 4 + y.numel() * 4 for a, y in host)
+        d2h = sum(o.numel() * 4 for o in outs)
+        e2e = {"value": round(e2e_ms * 1000, 1), "unit": "us", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        if rank == 0 and ws == 1 and not args.no_cpu:
+            threads = os.cpu_count() or 1
+            torch.set_num_threads(threads)
+            sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+            cpairs = [inputs.rbf_kernel_batch(b, n, seed=s, device="cpu") for (b, n), s in zip(sample, wl["seeds"])]
+
+            def cpu_step():
+                for a, y in cpairs:
+                    aa = a.detach().requires_grad_(True)
+                    lc = torch.linalg.cholesky(aa)
+                    al = torch.linalg.solve_triangular(lc, y.unsqueeze(-1), upper=False).squeeze(-1)
+                    (0.5 * (al * al).sum(-1) + torch.log(torch.diagonal(lc, dim1=-2, dim2=-1)).sum(-1)).sum().backward()
+
+            cpu_step()
+            t0 = time.perf_counter()
+            cpu_step()
+            dt = time.perf_counter() - t0
+            scale = sum(b * n**3 for b, n in wl["shapes"]) / sum(b * n**3 for b, n in sample)
+            cpu = {
+                "value": round(dt * 1e6 * scale, 1),
+                "unit": "us",
+                "cores": threads,
+                "kind": "port",
+                "sample": "torch CPU FP32 autograd of the same loss (cholesky, solve_triangular, log-diagonal) on "
+                + " + ".join(f"{b}x{n}" for b, n in sample)
+                + f", scaled by sum b n^3 x{scale:.2f}",
+            }
+    if rank == 0:
+        line = {
+            "metric": wl["metric"],
+            "value": round(ms * 1000, 1),
+            "unit": "us",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": wl["desc"],
+                "shapes": [f"{b}x{n}" for b, n in wl["shapes"]],
+                "mode": "forward fp32, adjoint bf16x3 (gp_nll defaults)",
+                "l2": "inputs larger than L2 (8x2048 is 128 MB); no flush",
+                "timing": "eager autograd calls (forward and backward), CUDA events, max over ranks",
+                "parallelism": f"weak scaling, {ws} rank(s) each a full step",
+            },
+            **extra,
+            "roofline": roof,
+            "kernels_one_step": {k: {"launches": c, "ms": round(t, 4)} for k, (c, t) in sorted(totals.items())},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args) -> int:
     wl0 = WORKLOADS[args.workload]
     if wl0.get("ragged"):
         return run_ours_ragged(args, wl0)
+    if wl0.get("gp"):
+        return run_ours_gp(args, wl0)
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
