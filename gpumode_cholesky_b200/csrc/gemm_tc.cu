@@ -165,11 +165,13 @@ __global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(GemmArgs g, int t
   uint32_t parity = 0;
   bool ok = true;
   int64_t b = blockIdx.y;
-  for (; b < g.batch && ok; b += gridDim.y) {
-    const float* X = g.x + b * g.sx;
-    const float* Y = g.y + b * g.sy;
-    float* C = g.c + b * g.sc;
-    const float* Cin = (g.c_in ? g.c_in : g.c) + b * g.sc;
+  const int64_t nb2 = g.batch2 > 0 ? g.batch2 : 1;
+  for (; b < g.batch * nb2 && ok; b += gridDim.y) {
+    const int64_t b1 = b / nb2, b2 = b - (b / nb2) * nb2;
+    const float* X = g.x + b1 * g.sx + b2 * g.sx2;
+    const float* Y = g.y + b1 * g.sy + b2 * g.sy2;
+    float* C = g.c + b1 * g.sc + b2 * g.sc2;
+    const float* Cin = (g.c_in ? g.c_in : g.c) + b1 * g.sc + b2 * g.sc2;
     bool any = false;
     for (int k0 = klo; k0 < khi; k0 += kGK) {
       // A operand: rows m (op1(X)[m][k]); B operand: rows n (op2(Y)[k][n]).
@@ -231,11 +233,258 @@ __global__ void __launch_bounds__(kGThreads, 1) gemm_tc_kernel(GemmArgs g, int t
   if (warp == 0) umma::tmem_dealloc(tmem, kGT);
 }
 
+// ---- packed operands + bulk-copy pipeline ----------------------------------------
+// Packed operand layout, per batch item: block (row tile t, K chunk c) of
+// 32 KB at ((t * tiles_k) + c) * 32 KB -- exactly the shared-memory image
+// g_stage writes (BF16 hi at +0 and lo at +16 KB, or the two TF32 K-halves),
+// zero-filled beyond the matrix.
+constexpr int kGStages = 3;
+constexpr size_t kGStage = 2 * kGOperand;  // A + B
+constexpr size_t kGBulkSmem = kGStages * kGStage + 1024 + 128;
+
+size_t gemm_pack_bytes(int64_t batch, int rows, int kdim) {
+  return (size_t)batch * (size_t)((rows + kGT - 1) / kGT) * (size_t)((kdim + kGK - 1) / kGK) * kGOperand;
+}
+
+// One 32 KB block (row tile, K chunk) per CTA; thread = (row r, 16-wide K
+// part p), so that four threads share a row and the CTA keeps many loads in
+// flight.  Reads are coalesced in either orientation (row-major: 64 bytes of
+// one row per thread; transposed: consecutive rows across a warp).
+constexpr int kPThreads = 512;
+
+template <int MODE>
+__global__ void __launch_bounds__(kPThreads) gemm_pack_kernel(const float* __restrict__ mat, int64_t s1, int64_t s2,
+                                                              int64_t nb2, int ld, int rowmajor, int rows, int kdim,
+                                                              int tiles_k, int64_t items, uint8_t* __restrict__ out) {
+  const int tr = blockIdx.x / tiles_k, tk = blockIdx.x - (blockIdx.x / tiles_k) * tiles_k;
+  const int r = threadIdx.x & 127, p = threadIdx.x >> 7;
+  const int i = tr * kGT + r, k0 = tk * kGK + 16 * p;
+  const size_t per = (size_t)((rows + kGT - 1) / kGT) * tiles_k * kGOperand;
+  for (int64_t b = blockIdx.y; b < items; b += gridDim.y) {
+    const int64_t b1 = b / nb2, b2 = b - (b / nb2) * nb2;
+    const float* M = mat + b1 * s1 + b2 * s2;
+    float v[16];
+    if (rowmajor) {
+      const float* src = M + (size_t)i * ld + k0;
+      if (i < rows && k0 + 16 <= kdim && ((reinterpret_cast<uintptr_t>(src) & 15u) == 0)) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 t = __ldg(reinterpret_cast<const float4*>(src) + q);
+          v[4 * q] = t.x;
+          v[4 * q + 1] = t.y;
+          v[4 * q + 2] = t.z;
+          v[4 * q + 3] = t.w;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = (i < rows && k0 + q < kdim) ? __ldg(src + q) : 0.0f;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = (i < rows && k0 + q < kdim) ? __ldg(M + (size_t)(k0 + q) * ld + i) : 0.0f;
+    }
+    uint8_t* op = out + b * per + (size_t)blockIdx.x * kGOperand;
+    if (MODE == B2P_MODE_TF32) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int Q = 4 * p + q;  // float4 index within the 64-wide row
+        const float4 t = make_float4(g_round_tf32(v[4 * q]), g_round_tf32(v[4 * q + 1]), g_round_tf32(v[4 * q + 2]),
+                                     g_round_tf32(v[4 * q + 3]));
+        *reinterpret_cast<float4*>(op + (Q >> 3) * 16384 + umma::sw128_offset(r, Q & 7)) = t;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          __nv_bfloat16 h0, l0, h1, l1;
+          umma::split_bf16(v[8 * c + 2 * q], h0, l0);
+          umma::split_bf16(v[8 * c + 2 * q + 1], h1, l1);
+          hi[q] = umma::pack_bf16(h0, h1);
+          lo[q] = umma::pack_bf16(l0, l1);
+        }
+        const uint32_t off = umma::sw128_offset(r, 2 * p + c);
+        *reinterpret_cast<uint4*>(op + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(op + 16384 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+      }
+    }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kGThreads, 1) gemm_bulk_kernel(GemmArgs g, int tiles_n, int32_t* err) {
+  extern __shared__ unsigned char graw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(graw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + kGStages * kGStage);  // [kGStages]
+  uint64_t* empty = full + kGStages;                                         // [kGStages]
+  uint64_t* done = empty + kGStages;                                         // [1]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* flag = reinterpret_cast<volatile int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  int tm, tn;
+  if (g.lower_out) {
+    const int q = blockIdx.x;
+    tm = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+    while ((tm + 1) * (tm + 2) / 2 <= q) ++tm;
+    while (tm * (tm + 1) / 2 > q) --tm;
+    tn = q - tm * (tm + 1) / 2;
+  } else {
+    tm = blockIdx.x / tiles_n;
+    tn = blockIdx.x - tm * tiles_n;
+  }
+  const int m0 = tm * kGT, n0 = tn * kGT;
+  int klo = 0, khi = g.k;
+  if (g.x_tri == 1) khi = min(khi, m0 + kGT);
+  if (g.x_tri == 2) klo = max(klo, m0);
+  if (g.y_tri == 1) klo = max(klo, n0);
+  if (g.y_tri == 2) khi = min(khi, n0 + kGT);
+  const int kc0 = klo / kGK, kc1 = khi > klo ? (khi + kGK - 1) / kGK : kc0;
+  const int nch = kc1 - kc0;
+  const int tiles_k = (g.k + kGK - 1) / kGK;
+  const size_t per_x = (size_t)((g.m + kGT - 1) / kGT) * tiles_k * kGOperand;
+  const size_t per_y = (size_t)((g.n + kGT - 1) / kGT) * tiles_k * kGOperand;
+
+  if (tid == 0) *flag = 0;
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, kGT);
+    umma::tmem_relinquish();
+  }
+  if (tid == 32) {
+    for (int i = 0; i < 2 * kGStages + 1; ++i) umma::mbar_init(full + i, 1);
+    umma::mbar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  uint32_t gload = 0, guse = 0, ph_done = 0;  // chunk counters over all items (thread 0), done parity
+  bool ok = true;
+  const int64_t nb2 = g.batch2 > 0 ? g.batch2 : 1;
+  for (int64_t b = blockIdx.y; b < g.batch * nb2 && ok; b += gridDim.y) {
+    const int64_t b1 = b / nb2, b2 = b - (b / nb2) * nb2;
+    float* C = g.c + b1 * g.sc + b2 * g.sc2;
+    const float* Cin = (g.c_in ? g.c_in : g.c) + b1 * g.sc + b2 * g.sc2;
+    const uint8_t* PX = g.pack_x + b * per_x + (size_t)tm * tiles_k * kGOperand;
+    const uint8_t* PY = g.pack_y + b * per_y + (size_t)tn * tiles_k * kGOperand;
+    if (nch > 0) {
+      if (tid == 0) {
+        bool pok = true;
+        const uint32_t first = gload;
+        auto load = [&](int i) -> bool {
+          const uint32_t st = gload % kGStages;
+          if (gload >= (uint32_t)kGStages &&
+              !umma::mbar_wait_bounded(empty + st, ((gload / kGStages) - 1u) & 1u, kGPolls))
+            return false;
+          uint8_t* dst = base + st * kGStage;
+          umma::mbar_arrive_expect_tx(full + st, (uint32_t)(2 * kGOperand));
+          umma::bulk_g2s(dst, PX + (size_t)(kc0 + i) * kGOperand, (uint32_t)kGOperand, full + st);
+          umma::bulk_g2s(dst + kGOperand, PY + (size_t)(kc0 + i) * kGOperand, (uint32_t)kGOperand, full + st);
+          ++gload;
+          return true;
+        };
+        for (int i = 0; i < kGStages && i < nch && pok; ++i) pok = load(i);
+        for (int i = 0; i < nch && pok; ++i) {
+          const uint32_t st = guse % kGStages;
+          if (!umma::mbar_wait_bounded(full + st, (guse / kGStages) & 1u, kGPolls)) {
+            pok = false;
+            break;
+          }
+          ++guse;
+          umma::fence_after_sync();
+          const uint32_t sa = umma::smem_u32(base + st * kGStage);
+          g_mmas<MODE>(tmem, sa, sa + (uint32_t)kGOperand, i > 0);
+          umma::mma_commit(empty + st);
+          if (i + kGStages < nch) pok = load(i + kGStages);
+        }
+        if (!pok) {
+          // Copies still in flight land before anything leaves.
+          for (uint32_t c = guse; c < gload; ++c)
+            umma::mbar_wait_bounded(full + (c % kGStages), (c / kGStages) & 1u, kGPolls);
+          guse = gload;
+          *flag = 1;
+        }
+        (void)first;
+        umma::mma_commit(done);
+      }
+      const bool got = umma::mbar_wait_bounded(done, ph_done, kGPolls);
+      ph_done ^= 1u;
+      umma::fence_after_sync();
+      if (!got) *flag = 1;
+      __syncthreads();
+      if (*flag) {
+        ok = false;
+        break;
+      }
+    }
+    // Epilogue: row i = m0 + 32*warp + lane, 4 chunks of 32 columns.
+    const int i = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int ch = 0; ch < 4; ++ch) {
+      float v[32];
+      if (nch > 0) {
+        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * ch), v);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) v[e] = 0.0f;
+      }
+      if (i < g.m) {
+        float* crow = C + (size_t)i * g.ldc;
+        const float* cin = Cin + (size_t)i * g.ldc;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          const int j = n0 + 32 * ch + e;
+          if (j < g.n && (!g.lower_out || j <= i)) {
+            float r = g.alpha * v[e];
+            if (g.phi) r = (j > i) ? 0.0f : (j == i ? 0.5f * r : r);
+            if (g.beta != 0.0f) r += g.beta * cin[j];
+            crow[j] = r;
+          }
+        }
+      }
+    }
+    // TMEM is rewritten by the next item's MMAs.
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  if (!ok && tid == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
+  if (!ok) umma::mbar_wait_bounded(done, ph_done ^ 1u, kGPolls);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kGT);
+}
+
+template <int MODE>
+static int launch_gemm_packed(const GemmArgs& g, int32_t* err, cudaStream_t s, int slot_bulk) {
+  const int tm = (g.m + kGT - 1) / kGT, tn = (g.n + kGT - 1) / kGT, tk = (g.k + kGK - 1) / kGK;
+  const int64_t nb2 = g.batch2 > 0 ? g.batch2 : 1;
+  const int64_t items = g.batch * nb2;
+  const unsigned by = (unsigned)std::min<int64_t>(items, 65535);
+  {
+    TraceScope ts(kKBwdGemm, s);
+    gemm_pack_kernel<MODE><<<dim3(tm * tk, by), kPThreads, 0, s>>>(g.x, g.sx, g.sx2, nb2, g.ldx, !g.trans_x, g.m,
+                                                                    g.k, tk, items, g.pack_x);
+    gemm_pack_kernel<MODE><<<dim3(tn * tk, by), kPThreads, 0, s>>>(g.y, g.sy, g.sy2, nb2, g.ldy, g.trans_y, g.n,
+                                                                    g.k, tk, items, g.pack_y);
+    if (int st = check_launch("gemm_pack_kernel")) return st;
+  }
+  if (int st = ensure_smem_attr((const void*)gemm_bulk_kernel<MODE>, kGBulkSmem, slot_bulk)) return st;
+  const int tiles = g.lower_out ? tm * (tm + 1) / 2 : tm * tn;
+  TraceScope ts(kKBwdGemm, s);
+  gemm_bulk_kernel<MODE><<<dim3(tiles, by), kGThreads, kGBulkSmem, s>>>(g, tn, err);
+  return check_launch("gemm_bulk_kernel");
+}
+
 int launch_gemm_tc(const GemmArgs& g, int mode, int32_t* err, cudaStream_t s) {
   if (g.batch <= 0 || g.m <= 0 || g.n <= 0) return B2P_OK;
+  if (g.pack_x != nullptr && g.pack_y != nullptr && g.k > 0) {
+    if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) return launch_gemm_packed<B2P_MODE_TF32>(g, err, s, kSlotBwdBulk0);
+    return launch_gemm_packed<B2P_MODE_BF16X3>(g, err, s, kSlotBwdBulk1);
+  }
   const int tm = (g.m + kGT - 1) / kGT, tn = (g.n + kGT - 1) / kGT;
   const int tiles = g.lower_out ? tm * (tm + 1) / 2 : tm * tn;
-  const dim3 grid(tiles, (unsigned)std::min<int64_t>(g.batch, 65535));
+  const dim3 grid(tiles, (unsigned)std::min<int64_t>(g.batch * (g.batch2 > 0 ? g.batch2 : 1), 65535));
   TraceScope ts(kKBwdGemm, s);
   if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)gemm_tc_kernel<B2P_MODE_TF32>, kGSmem, kSlotBwd0)) return st;

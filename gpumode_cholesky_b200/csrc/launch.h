@@ -88,8 +88,20 @@ struct GemmArgs {
   float alpha, beta;
   int64_t batch;
   const float* c_in;     // C read from here (null: from c); same layout as c
+  // Optional scratch (both or neither, gemm_pack_bytes each): op1(X) and
+  // op2(Y) are first packed once into the MMA's tile image, and the product
+  // streams the tiles with bulk copies instead of converting every operand
+  // row in every output tile.
+  uint8_t* pack_x;
+  uint8_t* pack_y;
+  // Optional second batch dimension (0 = none): item (b, b2) of C starts at
+  // c + b sc + b2 sc2 (likewise x, y), b2 < batch2.
+  int64_t batch2;
+  int64_t sx2, sy2, sc2;
 };
 int launch_gemm_tc(const GemmArgs& g, int mode, int32_t* err, cudaStream_t s);
+// Bytes of one packed operand of `rows` x `kdim` per batch item.
+size_t gemm_pack_bytes(int64_t batch, int rows, int kdim);
 
 // Cholesky adjoint (potrf_backward.cu).
 size_t backward_workspace_bytes(int64_t batch, int64_t n);
@@ -167,6 +179,8 @@ enum SmemSlot {
   kSlotSplitW0,
   kSlotSplitW1,
   kSlotBwdSmall,
+  kSlotBwdBulk0,
+  kSlotBwdBulk1,
   kSlotTrsv0,
   kSlotTrsv1,
   kSlotGpForward,

@@ -162,8 +162,16 @@ __global__ void __launch_bounds__(kBsThreads, 1)
   }
 }
 
-static GemmArgs gemm_args(int64_t batch, int n) {
+// Packed-operand scratch of the current call (see GemmArgs::pack_x).
+struct PackScratch {
+  uint8_t* x = nullptr;
+  uint8_t* y = nullptr;
+};
+
+static GemmArgs gemm_args(int64_t batch, int n, const PackScratch& ps) {
   GemmArgs g{};
+  g.pack_x = ps.x;
+  g.pack_y = ps.y;
   g.sx = g.sy = g.sc = (int64_t)n * n;
   g.ldx = g.ldy = g.ldc = n;
   g.alpha = 1.0f;
@@ -173,18 +181,24 @@ static GemmArgs gemm_args(int64_t batch, int n) {
   return g;
 }
 
-// U[lo:hi, lo:hi] = inverse of L[lo:hi, lo:hi] (block indices, 64 wide);
-// diagonal blocks are already inverted.  tmp holds L21 U11.
-static int trtri_rec(const float* l, float* u, float* tmp, int64_t batch, int n, int lo, int hi, int mode,
-                     int32_t* err, cudaStream_t s) {
-  if (hi - lo <= 1) return B2P_OK;
-  const int mid = (lo + hi) / 2;
-  if (int st = trtri_rec(l, u, tmp, batch, n, lo, mid, mode, err, s)) return st;
-  if (int st = trtri_rec(l, u, tmp, batch, n, mid, hi, mode, err, s)) return st;
+// Packing pays once both sides of a product are this large.
+constexpr int kPackMin = 256;
+
+// The off-diagonal block of `pairs` block pairs ([lo, mid), [mid, hi), then
+// the same shape every 2 (mid - lo) blocks down the diagonal), each of whose
+// diagonal halves is already inverted: U21 = -U22 (L21 U11); tmp holds
+// L21 U11.  One batched product per step for all pairs.
+static int trtri_combine(const float* l, float* u, float* tmp, int64_t batch, int n, int lo, int mid, int hi,
+                         int64_t pairs, int mode, int32_t* err, const PackScratch& ps, cudaStream_t s) {
   const int r0 = lo * 64, r1 = mid * 64, r2 = std::min(hi * 64, n);
   const size_t o21 = (size_t)r1 * n + r0, o11 = (size_t)r0 * n + r0, o22 = (size_t)r1 * n + r1;
+  const int64_t step = 2LL * (r1 - r0) * (n + 1);  // next pair along the diagonal
+  const PackScratch none;
+  const PackScratch& pk = (r2 - r1 >= kPackMin && r1 - r0 >= kPackMin) ? ps : none;
   // tmp21 = L21 * U11   (U11 lower: op2(Y)[k][c] nonzero for k >= c)
-  GemmArgs g = gemm_args(batch, n);
+  GemmArgs g = gemm_args(batch, n, pk);
+  g.batch2 = pairs;
+  g.sx2 = g.sy2 = g.sc2 = step;
   g.x = l + o21;
   g.y = u + o11;
   g.c = tmp + o21;
@@ -194,7 +208,9 @@ static int trtri_rec(const float* l, float* u, float* tmp, int64_t batch, int n,
   g.y_tri = 1;
   if (int st = launch_gemm_tc(g, mode, err, s)) return st;
   // U21 = -U22 * tmp21   (U22 lower: op1(X)[m][k] nonzero for k <= m)
-  g = gemm_args(batch, n);
+  g = gemm_args(batch, n, pk);
+  g.batch2 = pairs;
+  g.sx2 = g.sy2 = g.sc2 = step;
   g.x = u + o22;
   g.y = tmp + o21;
   g.c = u + o21;
@@ -206,8 +222,48 @@ static int trtri_rec(const float* l, float* u, float* tmp, int64_t batch, int n,
   return launch_gemm_tc(g, mode, err, s);
 }
 
+// U[lo:lo+len, lo:lo+len] for a power-of-two number of 64-wide blocks, bottom
+// up: at width h every aligned pair of h-block inverses merges into one of
+// 2h blocks, all pairs of a level in one batched product.  A pair that holds
+// the last (partial) block of the matrix has its own product.
+static int trtri_pow2(const float* l, float* u, float* tmp, int64_t batch, int n, int nblk, int lo, int len, int mode,
+                      int32_t* err, const PackScratch& ps, cudaStream_t s) {
+  for (int h = 1; 2 * h <= len; h *= 2) {
+    const int pairs = len / (2 * h);
+    const bool partial = (lo + len == nblk) && (n % 64) != 0;
+    const int full = partial ? pairs - 1 : pairs;
+    if (full > 0) {
+      if (int st = trtri_combine(l, u, tmp, batch, n, lo, lo + h, lo + 2 * h, full, mode, err, ps, s)) return st;
+    }
+    if (partial) {
+      const int j0 = lo + (pairs - 1) * 2 * h;
+      if (int st = trtri_combine(l, u, tmp, batch, n, j0, j0 + h, j0 + 2 * h, 1, mode, err, ps, s)) return st;
+    }
+  }
+  return B2P_OK;
+}
+
+// U[lo:hi, lo:hi] = inverse of L[lo:hi, lo:hi] (block indices, 64 wide);
+// diagonal blocks are already inverted.  Splits off the largest power-of-two
+// prefix (batched levels), recurses on the rest, then merges the two.
+static int trtri_range(const float* l, float* u, float* tmp, int64_t batch, int n, int nblk, int lo, int hi, int mode,
+                       int32_t* err, const PackScratch& ps, cudaStream_t s) {
+  const int len = hi - lo;
+  if (len <= 1) return B2P_OK;
+  if ((len & (len - 1)) == 0) return trtri_pow2(l, u, tmp, batch, n, nblk, lo, len, mode, err, ps, s);
+  int p = 1;
+  while (2 * p < len) p *= 2;
+  if (int st = trtri_pow2(l, u, tmp, batch, n, nblk, lo, p, mode, err, ps, s)) return st;
+  if (int st = trtri_range(l, u, tmp, batch, n, nblk, lo + p, hi, mode, err, ps, s)) return st;
+  return trtri_combine(l, u, tmp, batch, n, lo, lo + p, hi, 1, mode, err, ps, s);
+}
+
+// U and one temporary (batch x n x n FP32 each), then the two packed operands
+// of the tensor-core products (1024-byte aligned).
 size_t backward_workspace_bytes(int64_t batch, int64_t n) {
-  return n <= 128 ? 0 : (size_t)2 * batch * n * n * sizeof(float);
+  if (n <= 128) return 0;
+  const size_t pack = (gemm_pack_bytes(batch, (int)n, (int)n) + 1023) & ~(size_t)1023;
+  return (size_t)2 * batch * n * n * sizeof(float) + 2 * pack + 1024;
 }
 
 int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch, int n, int mode, void* ws,
@@ -229,6 +285,13 @@ int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch
   const size_t mat = (size_t)batch * n * n;
   float* u = static_cast<float*>(ws);
   float* w1 = u + mat;
+  PackScratch ps;
+  {
+    const size_t pack = (gemm_pack_bytes(batch, n, n) + 1023) & ~(size_t)1023;
+    uint8_t* p0 = reinterpret_cast<uint8_t*>(((reinterpret_cast<uintptr_t>(w1 + mat)) + 1023) & ~(uintptr_t)1023);
+    ps.x = p0;
+    ps.y = p0 + pack;
+  }
   int32_t* err = nullptr;
   // U = L^{-1}: zero (upper part stays zero), diagonal blocks, recursion.
   if (cudaMemsetAsync(u, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
@@ -240,10 +303,12 @@ int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch
         l, u, batch, n);
   }
   if (int st = check_launch("trtri_diag_kernel")) return st;
-  if (int st = trtri_rec(l, u, w1, batch, n, 0, nblk, mode, err, s)) return st;
+  if (int st = trtri_range(l, u, w1, batch, n, nblk, 0, nblk, mode, err, ps, s)) return st;
+  const PackScratch none;
+  const PackScratch& pbig = n >= kPackMin ? ps : none;
   // P = Phi(tril(L^T Lbar)) into w1 (upper part zero).
   if (cudaMemsetAsync(w1, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
-  GemmArgs g = gemm_args(batch, n);
+  GemmArgs g = gemm_args(batch, n, pbig);
   g.x = l;
   g.y = lbar;
   g.c = w1;
@@ -256,7 +321,7 @@ int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch
   if (int st = launch_gemm_tc(g, mode, err, s)) return st;
   // Z = P U into abar (lower; upper zero).
   if (cudaMemsetAsync(abar, 0, mat * sizeof(float), s) != cudaSuccess) return check_launch("cudaMemsetAsync");
-  g = gemm_args(batch, n);
+  g = gemm_args(batch, n, pbig);
   g.x = w1;
   g.y = u;
   g.c = abar;
@@ -266,7 +331,7 @@ int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch
   g.lower_out = 1;
   if (int st = launch_gemm_tc(g, mode, err, s)) return st;
   // S = U^T Z into w1.
-  g = gemm_args(batch, n);
+  g = gemm_args(batch, n, pbig);
   g.x = u;
   g.y = abar;
   g.c = w1;
