@@ -15,6 +15,7 @@
 #include <mutex>
 
 #include "launch.h"
+#include "panel_copy.cuh"
 
 namespace b2p {
 
@@ -173,9 +174,25 @@ int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, i
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
+  const bool auto_path = path == B2P_PATH_AUTO;
   if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
   if (!path_supported(path, batch, n, mode))
     return set_error(B2P_ERR_UNSUPPORTED, "path %d does not support n=%lld mode 0x%x", path, (long long)n, mode);
+  if (auto_path && path == B2P_PATH_FUSED) {
+    // One CTA per matrix runs in waves of `per` matrices; when the last wave
+    // would be less than half full, those matrices run instead as clusters
+    // of CTAs each (same workspace layout, so they take their own slice).
+    const int64_t per = (int64_t)device_sms() * (n <= 512 ? 2 : 1);
+    const int64_t tail = batch % per;
+    if (batch > per && tail > 0 && tail * 2 <= per && fused_ws_supported(tail, n, mode)) {
+      const int64_t head = batch - tail;
+      if (int st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s)) return st;
+      const size_t moff = (size_t)head * (size_t)n * (size_t)n;
+      const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
+      return potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
+                            workspace_bytes - woff, info ? info + head : nullptr, s);
+    }
+  }
   return potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s);
 }
 
