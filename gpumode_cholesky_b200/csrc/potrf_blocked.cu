@@ -24,6 +24,7 @@
 // 5152-5196 e62 diagonal block + inverse panel multiply); here every step is
 // a kernel of this library.
 #include <algorithm>
+#include <mutex>
 
 #include "diag64.cuh"
 #include "launch.h"
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(kGemmThreads)
 // for the first block column and L afterwards, the result always goes to L.
 template <bool RAGGED>
 __global__ void __launch_bounds__(kGemmThreads)
-    trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0) {
+    trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0, int part) {
   extern __shared__ __align__(16) float tsm[];
   float* As = tsm;
   float* Bs = As + kNB * kGemmLd;
@@ -297,11 +298,22 @@ __global__ void __launch_bounds__(kGemmThreads)
     const int n = tg.n;
     int ti = tg.ti, tj = tg.tj;
     if (!RAGGED) {
+      // part 0: every lower tile; 1: the first tile column only (the next
+      // block column, for the look-ahead); 2: every lower tile but those.
       const int q = blockIdx.x;
-      ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
-      while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
-      while (ti * (ti + 1) / 2 > q) --ti;
-      tj = q - ti * (ti + 1) / 2;
+      if (part == 1) {
+        ti = q;
+        tj = 0;
+      } else {
+        ti = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+        while ((ti + 1) * (ti + 2) / 2 <= q) ++ti;
+        while (ti * (ti + 1) / 2 > q) --ti;
+        tj = q - ti * (ti + 1) / 2;
+        if (part == 2) {
+          ++ti;
+          ++tj;
+        }
+      }
     }
     const int t0 = k0 + kNB;
     const int i0 = t0 + ti * kTile, j0 = t0 + tj * kTile;
@@ -361,6 +373,35 @@ size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode) {
   return (size_t)batch * kNB * kNB * sizeof(float);
 }
 
+namespace {
+// Per device: the stream the FP32 look-ahead runs the bulk of each trailing
+// update on, with the events that fork it from and join it to the caller's.
+struct TrailStream {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t join = nullptr;
+};
+constexpr int kTrailDevices = 64;
+TrailStream g_trail[kTrailDevices];
+std::mutex g_trail_mu;
+
+int trail_stream(TrailStream** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kTrailDevices)
+    return set_error(B2P_ERR_CUDA, "no usable current device");
+  std::lock_guard<std::mutex> lock(g_trail_mu);
+  TrailStream& t = g_trail[dev];
+  if (t.stream == nullptr) {
+    cudaError_t e = cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "trail stream set-up: %s", cudaGetErrorString(e));
+  }
+  *out = &t;
+  return B2P_OK;
+}
+}  // namespace
+
 int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
                   size_t ws_bytes, int32_t* info, cudaStream_t s) {
   const int m = mode & B2P_MODE_MASK;
@@ -393,7 +434,16 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       }
       if (int st = check_launch("diag_kernel")) return st;
       const int R = n - k0 - kNB;
-      if (R <= 0) return B2P_OK;
+      if (R <= 0) {
+        // The FP32 look-ahead's stream rejoins the caller's before the end.
+        if (!tensor && k0 > K0) {
+          TrailStream* ts2 = nullptr;
+          if (int st = trail_stream(&ts2)) return st;
+          const cudaError_t e = cudaStreamWaitEvent(s, ts2->join, 0);
+          if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaStreamWaitEvent: %s", cudaGetErrorString(e));
+        }
+        return B2P_OK;
+      }
       const int T = (R + kTile - 1) / kTile;
       {
         TraceScope ts(kKPanel, s);
@@ -406,11 +456,30 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
           return st;
         continue;
       }
+      // FP32 look-ahead: the tiles of the next block column first (they are
+      // all diag and panel of step k+1 read), the rest on the side stream
+      // beside that step; step k+1's own update waits for the rest.
+      TrailStream* ts2 = nullptr;
+      if (int st = trail_stream(&ts2)) return st;
+      auto check = [](cudaError_t e, const char* what) -> int {
+        return e == cudaSuccess ? B2P_OK : set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+      };
+      if (k0 > K0) {
+        if (int st = check(cudaStreamWaitEvent(s, ts2->join, 0), "cudaStreamWaitEvent")) return st;
+      }
       {
         TraceScope ts(kKTrail, s);
-        trail_kernel<false><<<dim3(T * (T + 1) / 2, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0);
+        trail_kernel<false><<<dim3(T, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0, 1);
       }
       if (int st = check_launch("trail_kernel")) return st;
+      if (int st = check(cudaEventRecord(ts2->fork, s), "cudaEventRecord")) return st;
+      if (int st = check(cudaStreamWaitEvent(ts2->stream, ts2->fork, 0), "cudaStreamWaitEvent")) return st;
+      if (T > 1) {
+        TraceScope ts(kKTrail, ts2->stream);
+        trail_kernel<false><<<dim3(T * (T - 1) / 2, gy), kGemmThreads, tsmem, ts2->stream>>>(src, l, sch, k0, 2);
+        if (int st = check_launch("trail_kernel")) return st;
+      }
+      if (int st = check(cudaEventRecord(ts2->join, ts2->stream), "cudaEventRecord")) return st;
     }
     if (jmax < n) {
       // C[jmax:, jmax:] -= X X^T, X = L[jmax:, K0:jmax] (lower triangle only).
@@ -465,7 +534,7 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
     Sched sr = ragged_sched(t, t.items + st.trail_beg, st.ntrail);
     if (tensor) return launch_syrk_tc(src, l, sr, true, 0, k0, mode, info, s);
     TraceScope ts(kKTrail, s);
-    trail_kernel<true><<<(int)std::min<int64_t>(st.ntrail, 1 << 30), kGemmThreads, tsmem, s>>>(src, l, sr, k0);
+    trail_kernel<true><<<(int)std::min<int64_t>(st.ntrail, 1 << 30), kGemmThreads, tsmem, s>>>(src, l, sr, k0, 0);
   }
   return check_launch("trail_kernel<ragged>");
 }
