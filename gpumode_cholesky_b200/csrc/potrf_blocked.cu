@@ -282,15 +282,65 @@ __global__ void __launch_bounds__(kGemmThreads)
 // Trailing SYRK on lower 64x64 tiles.  The C tile is prefetched into shared
 // memory with cp.async while the panel tiles load and multiply; `csrc` is A
 // for the first block column and L afterwards, the result always goes to L.
+// The trailing update runs 256 threads per 64x64 tile (4x4 outputs per
+// thread: four times the warps of the 8x8 layout, for latency hiding at the
+// same shared-memory footprint).  Each output still accumulates m = 0..63 in
+// order with one fmaf per step, so results equal the 8x8 layout's bit for bit.
+constexpr int kTrailThreads = 256;
+
+// load_rows_t with 256 threads: thread (row t % 64, quarter t / 64) moves 16 values.
+__device__ __forceinline__ void load_rows_t256(const float* __restrict__ mat, int n, int row0, int col0,
+                                               float* dst) {
+  const int i = threadIdx.x & 63, q4 = threadIdx.x >> 6;
+  const bool ok = row0 + i < n;
+  if ((n & 3) == 0) {
+    const float4* src = reinterpret_cast<const float4*>(mat + (size_t)(ok ? row0 + i : 0) * n + col0) + 4 * q4;
+    float4 v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = ok ? src[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int m = 16 * q4 + 4 * q;
+      dst[(m + 0) * kGemmLd + i] = v[q].x;
+      dst[(m + 1) * kGemmLd + i] = v[q].y;
+      dst[(m + 2) * kGemmLd + i] = v[q].z;
+      dst[(m + 3) * kGemmLd + i] = v[q].w;
+    }
+  } else {
+    const float* src = mat + (size_t)(ok ? row0 + i : 0) * n + col0;
+#pragma unroll 16
+    for (int m = 16 * q4; m < 16 * q4 + 16; ++m) dst[m * kGemmLd + i] = ok ? src[m] : 0.0f;
+  }
+}
+
+// acc[r][c] = sum_m As[m][4ty + r] * Bs[m][4tx + c]
+__device__ __forceinline__ void tile_mma_4x4(const float* As, const float* Bs, int ty, int tx, float (&acc)[4][4]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0f;
+#pragma unroll 8
+  for (int m = 0; m < kNB; ++m) {
+    const float4 a = *reinterpret_cast<const float4*>(As + m * kGemmLd + 4 * ty);
+    const float4 b = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 4 * tx);
+    const float a4[4] = {a.x, a.y, a.z, a.w};
+    const float b4[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(a4[r], b4[c], acc[r][c]);
+  }
+}
+
 template <bool RAGGED>
-__global__ void __launch_bounds__(kGemmThreads)
+__global__ void __launch_bounds__(kTrailThreads)
     trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0, int part) {
   extern __shared__ __align__(16) float tsm[];
   float* As = tsm;
   float* Bs = As + kNB * kGemmLd;
   float* Cs = Bs + kNB * kGemmLd;  // [64][kGemmLd], row-major C tile
   const int tid = threadIdx.x;
-  const int ty = tid >> 3, tx = tid & 7;
+  const int ty = tid >> 4, tx = tid & 15;
   const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
   const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
   for (int64_t it = start; it < sch.count; it += stride) {
@@ -321,43 +371,40 @@ __global__ void __launch_bounds__(kGemmThreads)
     const size_t moff = tg.off;
     if (vec) {
 #pragma unroll
-      for (int it = 0; it < 16; ++it) {
-        const int e = tid + kGemmThreads * it;
+      for (int it = 0; it < 4; ++it) {
+        const int e = tid + kTrailThreads * it;
         const int r = e >> 4, c4 = e & 15;
         if (i0 + r < n) cp_async16(Cs + r * kGemmLd + 4 * c4, csrc + moff + (size_t)(i0 + r) * n + j0 + 4 * c4);
       }
       cp_async_commit();
     }
     float* mat = l + moff;
-    load_rows_t(mat, n, i0, k0, As);
-    if (ti != tj) load_rows_t(mat, n, j0, k0, Bs);
+    load_rows_t256(mat, n, i0, k0, As);
+    if (ti != tj) load_rows_t256(mat, n, j0, k0, Bs);
     __syncthreads();
-    float acc[8][8];
-    tile_mma_8x8(As, ti != tj ? Bs : As, ty, tx, acc);
+    float acc[4][4];
+    tile_mma_4x4(As, ti != tj ? Bs : As, ty, tx, acc);
     if (vec) cp_async_wait_all();
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int rl = slot_index(ty, r);
+    for (int r = 0; r < 4; ++r) {
+      const int rl = 4 * ty + r;
       const int i = i0 + rl;
       if (i < n) {
         float* row = mat + (size_t)i * n + j0;
         if (vec && ti != tj) {
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            float4 c = *reinterpret_cast<const float4*>(Cs + rl * kGemmLd + 32 * h + 4 * tx);
-            c.x -= acc[r][4 * h + 0];
-            c.y -= acc[r][4 * h + 1];
-            c.z -= acc[r][4 * h + 2];
-            c.w -= acc[r][4 * h + 3];
-            *reinterpret_cast<float4*>(row + 32 * h + 4 * tx) = c;
-          }
+          float4 c = *reinterpret_cast<const float4*>(Cs + rl * kGemmLd + 4 * tx);
+          c.x -= acc[r][0];
+          c.y -= acc[r][1];
+          c.z -= acc[r][2];
+          c.w -= acc[r][3];
+          *reinterpret_cast<float4*>(row + 4 * tx) = c;
         } else {
           const float* crow = csrc + moff + (size_t)i * n + j0;
 #pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const int jl = slot_index(tx, c);
-            if (j0 + jl <= i) row[jl] = (vec ? Cs[rl * kGemmLd + jl] : crow[jl]) - acc[r][c];
+          for (int c = 0; c < 4; ++c) {
+            const int jl = 4 * tx + c;
+            if (j0 + jl <= i && j0 + jl < n) row[jl] = (vec ? Cs[rl * kGemmLd + jl] : crow[jl]) - acc[r][c];
           }
         }
       }
@@ -469,14 +516,14 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       }
       {
         TraceScope ts(kKTrail, s);
-        trail_kernel<false><<<dim3(T, gy), kGemmThreads, tsmem, s>>>(src, l, sch, k0, 1);
+        trail_kernel<false><<<dim3(T, gy), kTrailThreads, tsmem, s>>>(src, l, sch, k0, 1);
       }
       if (int st = check_launch("trail_kernel")) return st;
       if (int st = check(cudaEventRecord(ts2->fork, s), "cudaEventRecord")) return st;
       if (int st = check(cudaStreamWaitEvent(ts2->stream, ts2->fork, 0), "cudaStreamWaitEvent")) return st;
       if (T > 1) {
         TraceScope ts(kKTrail, ts2->stream);
-        trail_kernel<false><<<dim3(T * (T - 1) / 2, gy), kGemmThreads, tsmem, ts2->stream>>>(src, l, sch, k0, 2);
+        trail_kernel<false><<<dim3(T * (T - 1) / 2, gy), kTrailThreads, tsmem, ts2->stream>>>(src, l, sch, k0, 2);
         if (int st = check_launch("trail_kernel")) return st;
       }
       if (int st = check(cudaEventRecord(ts2->join, ts2->stream), "cudaEventRecord")) return st;
@@ -534,7 +581,7 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
     Sched sr = ragged_sched(t, t.items + st.trail_beg, st.ntrail);
     if (tensor) return launch_syrk_tc(src, l, sr, true, 0, k0, mode, info, s);
     TraceScope ts(kKTrail, s);
-    trail_kernel<true><<<(int)std::min<int64_t>(st.ntrail, 1 << 30), kGemmThreads, tsmem, s>>>(src, l, sr, k0, 0);
+    trail_kernel<true><<<(int)std::min<int64_t>(st.ntrail, 1 << 30), kTrailThreads, tsmem, s>>>(src, l, sr, k0, 0);
   }
   return check_launch("trail_kernel<ragged>");
 }
