@@ -312,147 +312,199 @@ __global__ void __launch_bounds__(kPThreads) gemm_pack_kernel(const float* __res
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kGThreads, 1) gemm_bulk_kernel(GemmArgs g, int tiles_n, int32_t* err) {
-  extern __shared__ unsigned char graw[];
-  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(graw) + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(base + kGStages * kGStage);  // [kGStages]
-  uint64_t* empty = full + kGStages;                                         // [kGStages]
-  uint64_t* done = empty + kGStages;                                         // [1]
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-  volatile int* flag = reinterpret_cast<volatile int*>(tslot + 1);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+// Persistent, warp-specialized product over packed operands.  Warp 4 (one
+// thread) streams the packed 32 KB blocks through a 3-stage ring two chunks
+// ahead of the MMAs (across tile boundaries) and issues the MMAs of each
+// tile into one of two 128-column TMEM accumulators; warps 0-3 run the
+// epilogue of the previous tile from the other accumulator meanwhile.
+constexpr int kBEpi = 128;
+constexpr int kBThreads = kBEpi + 32;
 
+struct BulkTile {
+  int64_t b;    // flattened batch item
+  int m0, n0;   // output tile origin
+  int kc0, nch; // K chunks [kc0, kc0 + nch)
+};
+
+__device__ __forceinline__ BulkTile bulk_decode(const GemmArgs& g, int tiles, int tiles_n, int64_t w) {
+  BulkTile t;
+  const int q = (int)(w % tiles);
+  t.b = w / tiles;
   int tm, tn;
   if (g.lower_out) {
-    const int q = blockIdx.x;
     tm = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
     while ((tm + 1) * (tm + 2) / 2 <= q) ++tm;
     while (tm * (tm + 1) / 2 > q) --tm;
     tn = q - tm * (tm + 1) / 2;
   } else {
-    tm = blockIdx.x / tiles_n;
-    tn = blockIdx.x - tm * tiles_n;
+    tm = q / tiles_n;
+    tn = q - tm * tiles_n;
   }
-  const int m0 = tm * kGT, n0 = tn * kGT;
+  t.m0 = tm * kGT;
+  t.n0 = tn * kGT;
   int klo = 0, khi = g.k;
-  if (g.x_tri == 1) khi = min(khi, m0 + kGT);
-  if (g.x_tri == 2) klo = max(klo, m0);
-  if (g.y_tri == 1) klo = max(klo, n0);
-  if (g.y_tri == 2) khi = min(khi, n0 + kGT);
-  const int kc0 = klo / kGK, kc1 = khi > klo ? (khi + kGK - 1) / kGK : kc0;
-  const int nch = kc1 - kc0;
+  if (g.x_tri == 1) khi = min(khi, t.m0 + kGT);
+  if (g.x_tri == 2) klo = max(klo, t.m0);
+  if (g.y_tri == 1) klo = max(klo, t.n0);
+  if (g.y_tri == 2) khi = min(khi, t.n0 + kGT);
+  t.kc0 = klo / kGK;
+  t.nch = khi > klo ? (khi + kGK - 1) / kGK - t.kc0 : 0;
+  return t;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kBThreads, 1) gemm_bulk_kernel(GemmArgs g, int tiles_n, int tiles, int32_t* err) {
+  extern __shared__ unsigned char graw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(graw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + kGStages * kGStage);  // [kGStages]
+  uint64_t* empty = full + kGStages;                                         // [kGStages]
+  uint64_t* accf = empty + kGStages;                                         // [2] accumulator complete
+  uint64_t* accd = accf + 2;                                                 // [2] accumulator read out
+  uint64_t* fin = accd + 2;                                                  // [1] every MMA done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+  volatile int* flag = reinterpret_cast<volatile int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  const int64_t nb2 = g.batch2 > 0 ? g.batch2 : 1;
+  const int64_t W = (int64_t)tiles * g.batch * nb2;
   const int tiles_k = (g.k + kGK - 1) / kGK;
   const size_t per_x = (size_t)((g.m + kGT - 1) / kGT) * tiles_k * kGOperand;
   const size_t per_y = (size_t)((g.n + kGT - 1) / kGT) * tiles_k * kGOperand;
 
   if (tid == 0) *flag = 0;
   if (warp == 0) {
-    umma::tmem_alloc(tslot, kGT);
+    umma::tmem_alloc(tslot, 2 * kGT);
     umma::tmem_relinquish();
   }
   if (tid == 32) {
-    for (int i = 0; i < 2 * kGStages + 1; ++i) umma::mbar_init(full + i, 1);
+    for (int i = 0; i < 2 * kGStages + 2; ++i) umma::mbar_init(full + i, 1);  // full, empty, accf
+    for (int i = 0; i < 2; ++i) umma::mbar_init(accd + i, kBEpi / 32);
+    umma::mbar_init(fin, 1);
     umma::mbar_fence_init();
   }
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tslot;
-  uint32_t gload = 0, guse = 0, ph_done = 0;  // chunk counters over all items (thread 0), done parity
-  bool ok = true;
-  const int64_t nb2 = g.batch2 > 0 ? g.batch2 : 1;
-  for (int64_t b = blockIdx.y; b < g.batch * nb2 && ok; b += gridDim.y) {
-    const int64_t b1 = b / nb2, b2 = b - (b / nb2) * nb2;
-    float* C = g.c + b1 * g.sc + b2 * g.sc2;
-    const float* Cin = (g.c_in ? g.c_in : g.c) + b1 * g.sc + b2 * g.sc2;
-    const uint8_t* PX = g.pack_x + b * per_x + (size_t)tm * tiles_k * kGOperand;
-    const uint8_t* PY = g.pack_y + b * per_y + (size_t)tn * tiles_k * kGOperand;
-    if (nch > 0) {
-      if (tid == 0) {
-        bool pok = true;
-        const uint32_t first = gload;
-        auto load = [&](int i) -> bool {
-          const uint32_t st = gload % kGStages;
-          if (gload >= (uint32_t)kGStages &&
-              !umma::mbar_wait_bounded(empty + st, ((gload / kGStages) - 1u) & 1u, kGPolls))
-            return false;
-          uint8_t* dst = base + st * kGStage;
-          umma::mbar_arrive_expect_tx(full + st, (uint32_t)(2 * kGOperand));
-          umma::bulk_g2s(dst, PX + (size_t)(kc0 + i) * kGOperand, (uint32_t)kGOperand, full + st);
-          umma::bulk_g2s(dst + kGOperand, PY + (size_t)(kc0 + i) * kGOperand, (uint32_t)kGOperand, full + st);
-          ++gload;
-          return true;
-        };
-        for (int i = 0; i < kGStages && i < nch && pok; ++i) pok = load(i);
-        for (int i = 0; i < nch && pok; ++i) {
+
+  if (warp == kBEpi / 32) {
+    // ---------------- producer / MMA issuer ----------------
+    if (lane == 0) {
+      uint32_t gload = 0, guse = 0;
+      bool ok = true;
+      // Loader cursor: the next chunk to bring in (item lw, chunk lc).
+      int64_t lw = blockIdx.x;
+      int lc = 0;
+      BulkTile lt = lw < W ? bulk_decode(g, tiles, tiles_n, lw) : BulkTile{};
+      auto load_next = [&]() -> bool {
+        while (lw < W && lc >= lt.nch) {
+          lw += gridDim.x;
+          lc = 0;
+          if (lw < W) lt = bulk_decode(g, tiles, tiles_n, lw);
+        }
+        if (lw >= W) return true;  // nothing left to load
+        const uint32_t st = gload % kGStages;
+        if (gload >= (uint32_t)kGStages &&
+            !umma::mbar_wait_bounded(empty + st, ((gload / kGStages) - 1u) & 1u, kGPolls))
+          return false;
+        const int tm = lt.m0 / kGT, tn = lt.n0 / kGT;
+        const uint8_t* PX = g.pack_x + lt.b * per_x + ((size_t)tm * tiles_k + lt.kc0 + lc) * kGOperand;
+        const uint8_t* PY = g.pack_y + lt.b * per_y + ((size_t)tn * tiles_k + lt.kc0 + lc) * kGOperand;
+        uint8_t* dst = base + st * kGStage;
+        umma::mbar_arrive_expect_tx(full + st, (uint32_t)(2 * kGOperand));
+        umma::bulk_g2s(dst, PX, (uint32_t)kGOperand, full + st);
+        umma::bulk_g2s(dst + kGOperand, PY, (uint32_t)kGOperand, full + st);
+        ++gload;
+        ++lc;
+        return true;
+      };
+      for (int i = 0; i < kGStages - 1 && ok; ++i) ok = load_next();
+      uint32_t li = 0;
+      for (int64_t w = blockIdx.x; w < W && ok; w += gridDim.x, ++li) {
+        const BulkTile t = bulk_decode(g, tiles, tiles_n, w);
+        const uint32_t p = li & 1u;
+        // Accumulator p is free once the epilogue has read tile li - 2.
+        if (li >= 2 && !umma::mbar_wait_bounded(accd + p, ((li - 2) >> 1) & 1u, kGPolls)) {
+          ok = false;
+          break;
+        }
+        umma::fence_after_sync();
+        for (int i = 0; i < t.nch && ok; ++i) {
           const uint32_t st = guse % kGStages;
           if (!umma::mbar_wait_bounded(full + st, (guse / kGStages) & 1u, kGPolls)) {
-            pok = false;
+            ok = false;
             break;
           }
           ++guse;
           umma::fence_after_sync();
           const uint32_t sa = umma::smem_u32(base + st * kGStage);
-          g_mmas<MODE>(tmem, sa, sa + (uint32_t)kGOperand, i > 0);
+          g_mmas<MODE>(tmem + p * kGT, sa, sa + (uint32_t)kGOperand, i > 0);
           umma::mma_commit(empty + st);
-          if (i + kGStages < nch) pok = load(i + kGStages);
+          // Refill the stage of chunk guse - 2 (its MMAs ran before this one's).
+          ok = load_next();
         }
-        if (!pok) {
-          // Copies still in flight land before anything leaves.
-          for (uint32_t c = guse; c < gload; ++c)
-            umma::mbar_wait_bounded(full + (c % kGStages), (c / kGStages) & 1u, kGPolls);
-          guse = gload;
-          *flag = 1;
-        }
-        (void)first;
-        umma::mma_commit(done);
+        if (ok) umma::mma_commit(accf + p);
       }
-      const bool got = umma::mbar_wait_bounded(done, ph_done, kGPolls);
-      ph_done ^= 1u;
-      umma::fence_after_sync();
-      if (!got) *flag = 1;
-      __syncthreads();
-      if (*flag) {
-        ok = false;
+      if (!ok) {
+        // Copies still in flight land before anything leaves.
+        for (uint32_t c = guse; c < gload; ++c)
+          umma::mbar_wait_bounded(full + (c % kGStages), (c / kGStages) & 1u, kGPolls);
+        *flag = 1;
+      }
+      umma::mma_commit(fin);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: row i = m0 + 32 warp + lane ----------------
+    uint32_t li = 0;
+    for (int64_t w = blockIdx.x; w < W; w += gridDim.x, ++li) {
+      const BulkTile t = bulk_decode(g, tiles, tiles_n, w);
+      const uint32_t p = li & 1u;
+      const bool got = umma::mbar_wait_bounded(accf + p, (li >> 1) & 1u, kGPolls) && *flag == 0;
+      if (!__all_sync(0xffffffffu, got)) {
+        *flag = 1;
+        if (lane == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
         break;
       }
-    }
-    // Epilogue: row i = m0 + 32*warp + lane, 4 chunks of 32 columns.
-    const int i = m0 + 32 * warp + lane;
+      umma::fence_after_sync();
+      const int64_t b1 = t.b / nb2, b2 = t.b - (t.b / nb2) * nb2;
+      float* C = g.c + b1 * g.sc + b2 * g.sc2;
+      const float* Cin = (g.c_in ? g.c_in : g.c) + b1 * g.sc + b2 * g.sc2;
+      const int i = t.m0 + 32 * warp + lane;
 #pragma unroll 1
-    for (int ch = 0; ch < 4; ++ch) {
-      float v[32];
-      if (nch > 0) {
-        umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * ch), v);
-      } else {
+      for (int ch = 0; ch < 4; ++ch) {
+        float v[32];
+        if (t.nch > 0) {
+          umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + p * kGT + (uint32_t)(32 * ch), v);
+        } else {
 #pragma unroll
-        for (int e = 0; e < 32; ++e) v[e] = 0.0f;
-      }
-      if (i < g.m) {
-        float* crow = C + (size_t)i * g.ldc;
-        const float* cin = Cin + (size_t)i * g.ldc;
+          for (int e = 0; e < 32; ++e) v[e] = 0.0f;
+        }
+        if (i < g.m) {
+          float* crow = C + (size_t)i * g.ldc;
+          const float* cin = Cin + (size_t)i * g.ldc;
 #pragma unroll
-        for (int e = 0; e < 32; ++e) {
-          const int j = n0 + 32 * ch + e;
-          if (j < g.n && (!g.lower_out || j <= i)) {
-            float r = g.alpha * v[e];
-            if (g.phi) r = (j > i) ? 0.0f : (j == i ? 0.5f * r : r);
-            if (g.beta != 0.0f) r += g.beta * cin[j];
-            crow[j] = r;
+          for (int e = 0; e < 32; ++e) {
+            const int j = t.n0 + 32 * ch + e;
+            if (j < g.n && (!g.lower_out || j <= i)) {
+              float r = g.alpha * v[e];
+              if (g.phi) r = (j > i) ? 0.0f : (j == i ? 0.5f * r : r);
+              if (g.beta != 0.0f) r += g.beta * cin[j];
+              crow[j] = r;
+            }
           }
         }
       }
+      umma::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) umma::mbar_arrive(accd + p);
     }
-    // TMEM is rewritten by the next item's MMAs.
-    umma::fence_before_sync();
-    __syncthreads();
   }
-  if (!ok && tid == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
-  if (!ok) umma::mbar_wait_bounded(done, ph_done ^ 1u, kGPolls);
-  umma::fence_before_sync();
+  // Every MMA has completed before TMEM is released.
+  umma::mbar_wait_bounded(fin, 0u, kGPolls);
+  umma::fence_after_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, kGT);
+  if (warp == 0) umma::tmem_dealloc(tmem, 2 * kGT);
 }
 
 template <int MODE>
@@ -471,8 +523,10 @@ static int launch_gemm_packed(const GemmArgs& g, int32_t* err, cudaStream_t s, i
   }
   if (int st = ensure_smem_attr((const void*)gemm_bulk_kernel<MODE>, kGBulkSmem, slot_bulk)) return st;
   const int tiles = g.lower_out ? tm * (tm + 1) / 2 : tm * tn;
+  const int64_t work = (int64_t)tiles * items;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(work, (int64_t)device_sms()));
   TraceScope ts(kKBwdGemm, s);
-  gemm_bulk_kernel<MODE><<<dim3(tiles, by), kGThreads, kGBulkSmem, s>>>(g, tn, err);
+  gemm_bulk_kernel<MODE><<<grid, kBThreads, kGBulkSmem, s>>>(g, tn, tiles, err);
   return check_launch("gemm_bulk_kernel");
 }
 
