@@ -113,3 +113,23 @@ def test_custom_kernel_rejects_cpu_input():
         custom_kernel(torch.eye(4).expand(2, 4, 4).contiguous())
     with pytest.raises(TypeError):
         custom_kernel(torch.eye(4, dtype=torch.float64).expand(2, 4, 4).contiguous())
+
+
+def test_trsv_and_gp_argument_validation_without_device():
+    """The triangular-solve and GP entry points reject bad shapes and null
+    pointers before any launch, and accept empty batches."""
+    lib = _lib.load()
+    fake = ctypes.c_void_p(16)  # never dereferenced: every call below returns first
+    assert lib.b2p_trsv_batched(fake, fake, fake, 2, 40000, 0, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_trsv_batched(fake, fake, fake, -1, 8, 0, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_trsv_batched(None, fake, fake, 2, 8, 0, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_trsv_batched(None, None, None, 0, 8, 1, None) == _lib.B2P_OK
+    assert lib.b2p_trsv_batched(None, None, None, 4, 0, 1, None) == _lib.B2P_OK
+    assert lib.b2p_gp_nll_forward(fake, fake, fake, None, 2, 8, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_gp_nll_forward(fake, fake, fake, fake, 2, 32769, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_gp_nll_forward(None, None, None, None, 0, 8, None) == _lib.B2P_OK
+    assert lib.b2p_gp_nll_backward(fake, fake, None, fake, fake, 2, 8, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_gp_nll_backward(fake, fake, fake, fake, None, 2, 8, None) == _lib.B2P_ERR_INVALID_ARG
+    assert lib.b2p_gp_nll_backward(None, None, None, None, None, 0, 8, None) == _lib.B2P_OK
+    assert lib.b2p_gp_nll_backward(fake, fake, fake, fake, None, 2, 8, None) == _lib.B2P_ERR_INVALID_ARG
+    assert b"null" in lib.b2p_last_error()
