@@ -51,15 +51,40 @@ __global__ void __launch_bounds__(kD64Threads) trtri_diag_kernel(const float* __
   }
 }
 
-// out = (s + s^T) / 2, one element pair per thread.
-__global__ void sym_kernel(const float* __restrict__ s, float* __restrict__ out, int64_t batch, int n) {
-  const int64_t total = batch * (int64_t)n * n;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = e / ((int64_t)n * n);
-    const int64_t r = e - b * (int64_t)n * n;
-    const int i = (int)(r / n), j = (int)(r - (int64_t)(r / n) * n);
+// out = (s + s^T) / 2 by 32 x 32 tile pairs: tiles (bi, bj) and (bj, bi),
+// bi >= bj, both read row-wise (coalesced) into shared memory, both written
+// row-wise.  256 threads: 32 columns x 8 rows per pass.
+constexpr int kSymThreads = 256;
+
+__global__ void __launch_bounds__(kSymThreads) sym_kernel(const float* __restrict__ s, float* __restrict__ out,
+                                                          int64_t batch, int n) {
+  __shared__ float t1[32][33], t2[32][33];
+  const int nt = (n + 31) / 32;
+  const int64_t pairs = (int64_t)nt * (nt + 1) / 2;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t item = blockIdx.x; item < batch * pairs; item += gridDim.x) {
+    const int64_t b = item / pairs;
+    const int q = (int)(item - b * pairs);
+    int bi = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+    while ((bi + 1) * (bi + 2) / 2 <= q) ++bi;
+    while (bi * (bi + 1) / 2 > q) --bi;
+    const int bj = q - bi * (bi + 1) / 2;
     const float* sb = s + b * (int64_t)n * n;
-    out[e] = 0.5f * (sb[(size_t)i * n + j] + sb[(size_t)j * n + i]);
+    float* ob = out + b * (int64_t)n * n;
+    for (int r = ty; r < 32; r += kSymThreads / 32) {
+      const int i1 = 32 * bi + r, j1 = 32 * bj + tx;  // tile (bi, bj)
+      const int i2 = 32 * bj + r, j2 = 32 * bi + tx;  // tile (bj, bi)
+      t1[r][tx] = (i1 < n && j1 < n) ? sb[(size_t)i1 * n + j1] : 0.0f;
+      t2[r][tx] = (i2 < n && j2 < n) ? sb[(size_t)i2 * n + j2] : 0.0f;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += kSymThreads / 32) {
+      const int i1 = 32 * bi + r, j1 = 32 * bj + tx;
+      if (i1 < n && j1 < n) ob[(size_t)i1 * n + j1] = 0.5f * (t1[r][tx] + t2[tx][r]);
+      const int i2 = 32 * bj + r, j2 = 32 * bi + tx;
+      if (bi != bj && i2 < n && j2 < n) ob[(size_t)i2 * n + j2] = 0.5f * (t2[r][tx] + t1[tx][r]);
+    }
+    __syncthreads();
   }
 }
 
@@ -342,8 +367,10 @@ int potrf_backward(const float* l, const float* lbar, float* abar, int64_t batch
   if (int st = launch_gemm_tc(g, mode, err, s)) return st;
   {
     TraceScope ts(kKBwdSym, s);
-    const int grid = (int)std::min<int64_t>((int64_t)((mat + 255) / 256), (int64_t)device_sms() * 32);
-    sym_kernel<<<grid, 256, 0, s>>>(w1, abar, batch, n);
+    const int nt = (n + 31) / 32;
+    const int64_t items = batch * ((int64_t)nt * (nt + 1) / 2);
+    const int grid = (int)std::min<int64_t>(items, (int64_t)device_sms() * 8);
+    sym_kernel<<<grid, kSymThreads, 0, s>>>(w1, abar, batch, n);
   }
   return check_launch("sym_kernel");
 }
