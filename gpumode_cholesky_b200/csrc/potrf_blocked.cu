@@ -155,137 +155,11 @@ __global__ void __launch_bounds__(kD64Threads, 3)
 }
 
 // -------------------------------------------------------------------------
-// 64x64 FP32 tile products with 64 threads, 8x8 outputs per thread.
-constexpr int kGemmThreads = 64;
-
-// Load rows row0..row0+63 (cols col0..col0+63) of an n x n matrix into
-// dst[m][i] (transposed, row stride kGemmLd).  Rows >= n load 0.  Every
-// load is issued before the first shared-memory store.
-__device__ __forceinline__ void load_rows_t(const float* __restrict__ mat, int n, int row0,
-                                            int col0, float* dst) {
-  const int i = threadIdx.x;
-  const bool ok = row0 + i < n;
-  if ((n & 3) == 0) {
-    const float4* src = reinterpret_cast<const float4*>(mat + (size_t)(ok ? row0 + i : 0) * n + col0);
-    float4 v[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = ok ? src[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      dst[(4 * q + 0) * kGemmLd + i] = v[q].x;
-      dst[(4 * q + 1) * kGemmLd + i] = v[q].y;
-      dst[(4 * q + 2) * kGemmLd + i] = v[q].z;
-      dst[(4 * q + 3) * kGemmLd + i] = v[q].w;
-    }
-  } else {
-    const float* src = mat + (size_t)(ok ? row0 + i : 0) * n + col0;
-#pragma unroll 16
-    for (int m = 0; m < kNB; ++m) dst[m * kGemmLd + i] = ok ? src[m] : 0.0f;
-  }
-}
-
-// Row/column owned by register slot r (0..7) of thread coordinate t (0..7):
-// {4t..4t+3} then {32+4t..32+4t+3}, so that the eight threads of a quarter
-// warp read 128 contiguous bytes (bank-conflict-free float4 loads).
-__device__ __forceinline__ int slot_index(int t, int r) { return (r < 4) ? 4 * t + r : 32 + 4 * t + (r - 4); }
-
-// acc[r][c] = sum_m As[m][slot(ty,r)] * Bs[m][slot(tx,c)]
-__device__ __forceinline__ void tile_mma_8x8(const float* As, const float* Bs, int ty, int tx,
-                                             float (&acc)[8][8]) {
-#pragma unroll
-  for (int r = 0; r < 8; ++r)
-#pragma unroll
-    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
-#pragma unroll 4
-  for (int m = 0; m < kNB; ++m) {
-    const float4 a0 = *reinterpret_cast<const float4*>(As + m * kGemmLd + 4 * ty);
-    const float4 a1 = *reinterpret_cast<const float4*>(As + m * kGemmLd + 32 + 4 * ty);
-    const float4 b0 = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 4 * tx);
-    const float4 b1 = *reinterpret_cast<const float4*>(Bs + m * kGemmLd + 32 + 4 * tx);
-    const float a8[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-    const float b8[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-      for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(a8[r], b8[c], acc[r][c]);
-  }
-}
-
-template <bool RAGGED>
-__global__ void __launch_bounds__(kGemmThreads)
-    panel_kernel(const float* __restrict__ src, float* __restrict__ l, Sched sch, int k0,
-                 const float* __restrict__ tws) {
-  __shared__ __align__(16) float Ps[kNB * kGemmLd];
-  __shared__ __align__(16) float Ts[kNB * kGemmLd];
-  const int tid = threadIdx.x;
-  const int ty = tid >> 3, tx = tid & 7;
-  const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
-  const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
-  for (int64_t it = start; it < sch.count; it += stride) {
-    const Target tg = resolve_tile<RAGGED>(sch, it);
-    const int n = tg.n;
-    const int row0 = k0 + kNB + tg.ti * kTile;
-    const size_t moff = tg.off;
-    const float* tb = tws + tg.pos * kNB * kNB;
-    // Ts[m][c] = T[c][m]: the diagonal kernel stored T^T row-major.
-    {
-      float4 tv[16];
-#pragma unroll
-      for (int it = 0; it < 16; ++it) tv[it] = __ldg(reinterpret_cast<const float4*>(tb) + tid + kGemmThreads * it);
-      load_rows_t(src + moff, n, row0, k0, Ps);
-#pragma unroll
-      for (int it = 0; it < 16; ++it) {
-        const int e = tid + kGemmThreads * it;
-        *reinterpret_cast<float4*>(Ts + (e >> 4) * kGemmLd + (e & 15) * 4) = tv[it];
-      }
-    }
-    __syncthreads();
-    float acc[8][8];
-    tile_mma_8x8(Ps, Ts, ty, tx, acc);
-    float* mat = l + moff;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = row0 + slot_index(ty, r);
-      if (i < n) {
-        float* dst = mat + (size_t)i * n + k0;
-        if ((n & 3) == 0) {
-          reinterpret_cast<float4*>(dst + 4 * tx)[0] = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
-          reinterpret_cast<float4*>(dst + 32 + 4 * tx)[0] = make_float4(acc[r][4], acc[r][5], acc[r][6], acc[r][7]);
-        } else {
-#pragma unroll
-          for (int c = 0; c < 8; ++c) dst[slot_index(tx, c)] = acc[r][c];
-        }
-      }
-    }
-    // Zero block ti of the strip: rows k0..k0+63, cols k0+64+64*ti .. +63.
-    {
-      const int c0 = k0 + kNB + tg.ti * kTile;
-      const int cw = min(kTile, n - c0);
-      float* zb = mat + (size_t)k0 * n + c0;
-      if ((n & 3) == 0) {
-        const int q4 = cw >> 2;
-        for (int e = tid; e < kNB * q4; e += kGemmThreads) {
-          const int r = e / q4, q = e - (e / q4) * q4;
-          reinterpret_cast<float4*>(zb + (size_t)r * n)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      } else {
-        for (int e = tid; e < kNB * cw; e += kGemmThreads) {
-          const int r = e / cw, c = e - (e / cw) * cw;
-          zb[(size_t)r * n + c] = 0.0f;
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Trailing SYRK on lower 64x64 tiles.  The C tile is prefetched into shared
-// memory with cp.async while the panel tiles load and multiply; `csrc` is A
-// for the first block column and L afterwards, the result always goes to L.
-// The trailing update runs 256 threads per 64x64 tile (4x4 outputs per
-// thread: four times the warps of the 8x8 layout, for latency hiding at the
-// same shared-memory footprint).  Each output still accumulates m = 0..63 in
-// order with one fmaf per step, so results equal the 8x8 layout's bit for bit.
+// The panel multiply and the trailing update run 256 threads per 64x64 tile
+// (4x4 outputs per thread: four times the warps of the 8x8 layout, for
+// latency hiding at the same shared-memory footprint).  Each output still
+// accumulates m = 0..63 in order with one fmaf per step, so results equal the
+// 8x8 layout's bit for bit.
 constexpr int kTrailThreads = 256;
 
 // load_rows_t with 256 threads: thread (row t % 64, quarter t / 64) moves 16 values.
@@ -332,6 +206,76 @@ __device__ __forceinline__ void tile_mma_4x4(const float* As, const float* Bs, i
   }
 }
 
+template <bool RAGGED>
+__global__ void __launch_bounds__(kTrailThreads)
+    panel_kernel(const float* __restrict__ src, float* __restrict__ l, Sched sch, int k0,
+                 const float* __restrict__ tws) {
+  __shared__ __align__(16) float Ps[kNB * kGemmLd];
+  __shared__ __align__(16) float Ts[kNB * kGemmLd];
+  const int tid = threadIdx.x;
+  const int ty = tid >> 4, tx = tid & 15;
+  const int64_t start = RAGGED ? blockIdx.x : blockIdx.y;
+  const int64_t stride = RAGGED ? gridDim.x : gridDim.y;
+  for (int64_t it = start; it < sch.count; it += stride) {
+    const Target tg = resolve_tile<RAGGED>(sch, it);
+    const int n = tg.n;
+    const int row0 = k0 + kNB + tg.ti * kTile;
+    const size_t moff = tg.off;
+    const float* tb = tws + tg.pos * kNB * kNB;
+    // Ts[m][c] = T[c][m]: the diagonal kernel stored T^T row-major.
+    {
+      float4 tv[4];
+#pragma unroll
+      for (int it = 0; it < 4; ++it) tv[it] = __ldg(reinterpret_cast<const float4*>(tb) + tid + kTrailThreads * it);
+      load_rows_t256(src + moff, n, row0, k0, Ps);
+#pragma unroll
+      for (int it = 0; it < 4; ++it) {
+        const int e = tid + kTrailThreads * it;
+        *reinterpret_cast<float4*>(Ts + (e >> 4) * kGemmLd + (e & 15) * 4) = tv[it];
+      }
+    }
+    __syncthreads();
+    float acc[4][4];
+    tile_mma_4x4(Ps, Ts, ty, tx, acc);
+    float* mat = l + moff;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = row0 + 4 * ty + r;
+      if (i < n) {
+        float* dst = mat + (size_t)i * n + k0;
+        if ((n & 3) == 0) {
+          reinterpret_cast<float4*>(dst + 4 * tx)[0] = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) dst[4 * tx + c] = acc[r][c];
+        }
+      }
+    }
+    // Zero block ti of the strip: rows k0..k0+63, cols k0+64+64*ti .. +63.
+    {
+      const int c0 = k0 + kNB + tg.ti * kTile;
+      const int cw = min(kTile, n - c0);
+      float* zb = mat + (size_t)k0 * n + c0;
+      if ((n & 3) == 0) {
+        const int q4 = cw >> 2;
+        for (int e = tid; e < kNB * q4; e += kTrailThreads) {
+          const int r = e / q4, q = e - (e / q4) * q4;
+          reinterpret_cast<float4*>(zb + (size_t)r * n)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      } else {
+        for (int e = tid; e < kNB * cw; e += kTrailThreads) {
+          const int r = e / cw, c = e - (e / cw) * cw;
+          zb[(size_t)r * n + c] = 0.0f;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Trailing SYRK on lower 64x64 tiles.  The C tile is prefetched into shared
+// memory with cp.async while the panel tiles load and multiply; `csrc` is A
+// for the first block column and L afterwards, the result always goes to L.
 template <bool RAGGED>
 __global__ void __launch_bounds__(kTrailThreads)
     trail_kernel(const float* __restrict__ csrc, float* __restrict__ l, Sched sch, int k0, int part) {
@@ -494,7 +438,7 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       const int T = (R + kTile - 1) / kTile;
       {
         TraceScope ts(kKPanel, s);
-        panel_kernel<false><<<dim3(T, gy), kGemmThreads, 0, s>>>(src, l, sch, k0, tws);
+        panel_kernel<false><<<dim3(T, gy), kTrailThreads, 0, s>>>(src, l, sch, k0, tws);
       }
       if (int st = check_launch("panel_kernel")) return st;
       if (k0 + kNB >= jmax) continue;
@@ -574,7 +518,7 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
   if (st.npanel > 0) {
     Sched sp = ragged_sched(t, t.items + st.panel_beg, st.npanel);
     TraceScope ts(kKPanel, s);
-    panel_kernel<true><<<(int)std::min<int64_t>(st.npanel, 1 << 30), kGemmThreads, 0, s>>>(src, l, sp, k0, tws);
+    panel_kernel<true><<<(int)std::min<int64_t>(st.npanel, 1 << 30), kTrailThreads, 0, s>>>(src, l, sp, k0, tws);
   }
   if (int e = check_launch("panel_kernel<ragged>")) return e;
   if (st.ntrail > 0) {
