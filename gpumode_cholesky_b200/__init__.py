@@ -7,7 +7,7 @@ behind a C ABI (``include/b200_potrf.h``), called from Python through ctypes.
 
 from ._lib import LaunchTrace, PotrfError
 from .autograd import CholeskyFunction, cholesky_differentiable, potrf_backward
-from .gp import gp_nll
+from .gp import gp_nll, trsv
 from .potrf import cholesky, custom_kernel
 
 __all__ = [
@@ -19,4 +19,5 @@ __all__ = [
     "custom_kernel",
     "gp_nll",
     "potrf_backward",
+    "trsv",
 ]
