@@ -179,6 +179,7 @@ enum SmemSlot {
   kSlotSplitW0,
   kSlotSplitW1,
   kSlotBwdSmall,
+  kSlotDiagF64,
   kSlotBwdBulk0,
   kSlotBwdBulk1,
   kSlotTrsv0,

@@ -358,6 +358,89 @@ __global__ void __launch_bounds__(kTrailThreads)
 }
 
 // -------------------------------------------------------------------------
+// B2P_FLAG_FP64_DIAG: the diagonal step in FP64.  Same contract as
+// diag_kernel (dense batches): the block's lower triangle (identity beyond
+// w = min(64, n - k0)) is factored right-looking in FP64 shared memory, the
+// inverse T = L_kk^{-1} follows by column substitution (thread c: column c),
+// and L_kk (zeros above) and T^T go out rounded to FP32; info takes the first
+// pivot that is not positive.  One CTA per matrix, 128 threads.
+constexpr int kD64fLd = 65;
+constexpr size_t kDiagF64Smem = 2 * 64 * kD64fLd * sizeof(double);
+
+__global__ void __launch_bounds__(kD64Threads) diag_kernel_f64(const float* __restrict__ src, float* __restrict__ l,
+                                                               Sched sch, int k0, float* __restrict__ tws,
+                                                               int32_t* __restrict__ info) {
+  extern __shared__ __align__(16) double dsm[];
+  double* S = dsm;               // [64][kD64fLd]: the block, then L_kk
+  double* Tm = dsm + 64 * kD64fLd;  // [64][kD64fLd]: T = L_kk^{-1} (lower)
+  __shared__ int sbad;
+  const int tid = threadIdx.x;
+  for (int64_t it = blockIdx.x; it < sch.count; it += gridDim.x) {
+    const Target tg = resolve_matrix<false>(sch, it);
+    const int n = tg.n;
+    const int64_t b = tg.pos;
+    const int w = min(kNB, n - k0);
+    const size_t moff = tg.off + (size_t)k0 * n + k0;
+    const float* in = src + moff;
+    float* base = l + moff;
+    for (int e = tid; e < 64 * 64; e += kD64Threads) {
+      const int r = e >> 6, c = e & 63;
+      double v = (r == c) ? 1.0 : 0.0;
+      if (r < w) v = (c <= r) ? (double)in[(size_t)r * n + c] : 0.0;
+      S[r * kD64fLd + c] = v;
+    }
+    if (tid == 0) sbad = -1;
+    __syncthreads();
+    for (int k = 0; k < 64; ++k) {
+      if (tid == 0) {
+        const double d = S[k * kD64fLd + k];
+        if (!(d > 0.0) && sbad < 0) sbad = k;
+        S[k * kD64fLd + k] = sqrt(d);
+      }
+      __syncthreads();
+      const double piv = S[k * kD64fLd + k];
+      for (int i = k + 1 + tid; i < 64; i += kD64Threads) S[i * kD64fLd + k] /= piv;
+      __syncthreads();
+      // S[i][j] -= S[i][k] S[j][k] for k < j <= i
+      const int m = 63 - k;
+      for (int e = tid; e < m * m; e += kD64Threads) {
+        const int i = k + 1 + e / m, j = k + 1 + e % m;
+        if (j <= i) S[i * kD64fLd + j] -= S[i * kD64fLd + k] * S[j * kD64fLd + k];
+      }
+      __syncthreads();
+    }
+    if (tid < 64) {
+      const int c = tid;
+      for (int i = 0; i < c; ++i) Tm[i * kD64fLd + c] = 0.0;
+      for (int i = c; i < 64; ++i) {
+        double acc = (i == c) ? 1.0 : 0.0;
+        for (int k = c; k < i; ++k) acc -= S[i * kD64fLd + k] * Tm[k * kD64fLd + c];
+        Tm[i * kD64fLd + c] = acc / S[i * kD64fLd + i];
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < 64 * 64; e += kD64Threads) {
+      const int r = e >> 6, c = e & 63;
+      if (r < w && c < w) base[(size_t)r * n + c] = (c <= r) ? (float)S[r * kD64fLd + c] : 0.0f;
+    }
+    // tws[m][c] = T[c][m]
+    float* tb = tws + b * kNB * kNB;
+    for (int e = tid; e < 64 * 64; e += kD64Threads) {
+      const int mm = e >> 6, c = e & 63;
+      tb[e] = (mm < w && c < w) ? (float)Tm[c * kD64fLd + mm] : 0.0f;
+    }
+    if (info != nullptr && tid == 0) {
+      const int bad = sbad;
+      if (k0 == 0)
+        info[tg.mat] = bad >= 0 ? bad + 1 : 0;
+      else if (bad >= 0 && info[tg.mat] == 0)
+        info[tg.mat] = k0 + bad + 1;
+    }
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------------------------
 size_t blocked_workspace_bytes(int64_t batch, int64_t n, int mode) {
   (void)n;
   (void)mode;
@@ -396,8 +479,8 @@ int trail_stream(TrailStream** out) {
 int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void* ws,
                   size_t ws_bytes, int32_t* info, cudaStream_t s) {
   const int m = mode & B2P_MODE_MASK;
-  if (m == B2P_MODE_FP8 || (mode & B2P_FLAG_FP64_DIAG))
-    return set_error(B2P_ERR_UNSUPPORTED, "mode 0x%x not available for n=%d", mode, n);
+  if (m == B2P_MODE_FP8) return set_error(B2P_ERR_UNSUPPORTED, "mode 0x%x not available for n=%d", mode, n);
+  const bool f64diag = (mode & B2P_FLAG_FP64_DIAG) != 0;
   const bool tensor = (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3);
   const size_t need = blocked_workspace_bytes(batch, n, mode);
   if (ws == nullptr || ws_bytes < need)
@@ -406,6 +489,9 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
   const int sms = device_sms();
   const size_t dsmem = sizeof(Diag64Smem);
   if (int st = ensure_smem_attr((const void*)diag_kernel<false>, dsmem, kSlotDiag)) return st;
+  if (f64diag) {
+    if (int st = ensure_smem_attr((const void*)diag_kernel_f64, kDiagF64Smem, kSlotDiagF64)) return st;
+  }
   const size_t tsmem = (size_t)3 * kNB * kGemmLd * sizeof(float);
   if (int st = ensure_smem_attr((const void*)trail_kernel<false>, tsmem, kSlotTrail)) return st;
   const int gy = (int)std::min<int64_t>(batch, kMaxGridY);
@@ -421,7 +507,10 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
       {
         TraceScope ts(kKDiag, s);
-        diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
+        if (f64diag)
+          diag_kernel_f64<<<dgrid, kD64Threads, kDiagF64Smem, s>>>(src, l, sch, k0, tws, info);
+        else
+          diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
       }
       if (int st = check_launch("diag_kernel")) return st;
       const int R = n - k0 - kNB;

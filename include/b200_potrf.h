@@ -44,15 +44,19 @@ extern "C" {
 #define B2P_ERR_TIMEOUT 5       /* a bounded device-side wait gave up         */
 
 /* ---- precision modes ------------------------------------------------------ *
- * The diagonal tiles and the panel solves are FP32 in every mode; the mode
- * selects the arithmetic of the trailing (Schur complement) updates.        */
+ * The diagonal tiles and the panel solves are FP32 in every mode (unless
+ * B2P_FLAG_FP64_DIAG); the mode selects the arithmetic of the trailing
+ * (Schur complement) updates.                                              */
 #define B2P_MODE_FP32 0    /* plain FP32 end to end (SIMT FMA)                 */
 #define B2P_MODE_TF32 1    /* trailing update on tcgen05 kind::tf32            */
 #define B2P_MODE_BF16X3 2  /* trailing update as hi*hi+hi*lo+lo*hi BF16 on tcgen05 */
 #define B2P_MODE_FP8 3     /* trailing update in per-tile scaled E4M3 (n>=16384) */
 #define B2P_MODE_MASK 0xff
-/* Flag OR-ed into the mode: factor diagonal tiles in FP64 and re-factor a
- * panel in plain FP32 when its FP64 residual check fails.                    */
+/* Flag OR-ed into the mode: for n > 128, factor and invert every 64 x 64
+ * diagonal tile in FP64 (rounded to FP32 on store).  Flagged calls take the
+ * blocked path (the fused, warp-specialized and split paths keep FP32
+ * diagonal tiles); orders <= 128 ignore the flag.  No counterpart exists in
+ * the reference.                                                             */
 #define B2P_FLAG_FP64_DIAG 0x100
 
 /* Library version as major*10000 + minor*100 + patch. */

@@ -133,3 +133,14 @@ def test_trsv_and_gp_argument_validation_without_device():
     assert lib.b2p_gp_nll_backward(None, None, None, None, None, 0, 8, None) == _lib.B2P_OK
     assert lib.b2p_gp_nll_backward(fake, fake, fake, fake, None, 2, 8, None) == _lib.B2P_ERR_INVALID_ARG
     assert b"null" in lib.b2p_last_error()
+
+
+def test_fp64_diag_flag_routes_to_blocked_workspace():
+    """A flagged tensor-mode call takes the blocked path: its workspace is the
+    blocked path's (one 64 x 64 FP32 inverse per matrix), not the panel copies."""
+    lib = _lib.load()
+    plain = lib.b2p_potrf_workspace_size(8, 512, _lib.MODE_BF16X3)
+    flagged = lib.b2p_potrf_workspace_size(8, 512, _lib.MODE_BF16X3 | _lib.FLAG_FP64_DIAG)
+    assert flagged == 8 * 64 * 64 * 4
+    assert plain != flagged
+    assert lib.b2p_potrf_workspace_size(8, 512, _lib.MODE_FP32 | _lib.FLAG_FP64_DIAG) == 8 * 64 * 64 * 4

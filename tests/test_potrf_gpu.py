@@ -102,3 +102,26 @@ def test_full_size_properties(batch, n):
     ld = l.double()
     r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - a.double()) / torch.linalg.matrix_norm(a.double())
     assert r.max().item() < 2e-6
+
+
+@pytest.mark.parametrize("mode", ["fp32+fp64diag", "bf16x3+fp64diag"])
+@pytest.mark.parametrize("batch,n", [(3, 129), (2, 200), (4, 512), (1, 1088)])
+def test_fp64_diagonal_tiles(mode, batch, n):
+    """B2P_FLAG_FP64_DIAG: the diagonal tiles factor and invert in FP64 on the
+    blocked path.  Checker pass, FP64 error no worse than 2x the plain mode's,
+    and the oracle's info for a matrix with a negative pivot."""
+    a = inputs.generate_input(batch, n, 2, 7000 + n, "dense", device="cpu")
+    ours = cholesky(a.cuda(), mode=mode).cpu().numpy()
+    plain = cholesky(a.cuda(), mode=mode.split("+")[0]).cpu().numpy()
+    ok, msg = oracle.check_implementation(a.numpy(), ours)
+    assert ok, msg
+    assert np.all(np.triu(ours, 1) == 0.0)
+    l64, _ = oracle.potrf_f64(a.numpy())
+    assert _rel_err(ours, l64).max() <= 2.0 * _rel_err(plain, l64).max() + 1e-7
+    bad = a.clone()
+    j = n - 5
+    bad[batch - 1, j, j] = -1.0
+    info = torch.full((batch,), -3, dtype=torch.int32, device="cuda")
+    cholesky(bad.cuda(), mode=mode, info=info)
+    want = oracle.potrf_f64(bad.numpy())[1]
+    assert np.array_equal(info.cpu().numpy(), want)
