@@ -174,3 +174,25 @@ def test_config4_full_size():
         a = buf[o : o + n * n].view(n, n).double()
         worst = max(worst, (torch.linalg.norm(l @ l.T - a) / torch.linalg.norm(a)).item())
     assert worst <= 1e-5
+
+
+def test_autotune_picks_a_working_plan():
+    """autotune times each candidate and returns the fastest plan, which
+    factors the buffer like any other plan."""
+    from gpumode_cholesky_b200.ragged import autotune
+
+    orders = [20, 90, 150, 260, 300, 700, 1100]
+    mats = [inputs.well_conditioned(1, n, seed=5 * n, device="cpu")[0] for n in orders]
+    buf, orders, offs = pack(mats, device="cuda")
+    cands = [
+        {"pad_step": 64, "pad_step_large": 128, "large_path": "split", "streams": 1},
+        {"pad_step": 128, "pad_step_large": 128, "large_path": "fused_ws", "streams": 2},
+    ]
+    plan, results = autotune(buf, orders, offs, mode="bf16x3", candidates=cands, reps=1)
+    assert len(results) == 2 and all(us > 0 for _, us in results)
+    best = min(results, key=lambda r: r[1])[0]
+    assert plan.options.pad_step == best["pad_step"] and plan.options.streams == best["streams"]
+    out = plan.factor(buf)
+    for m, l in zip(mats, unpack(out, orders, offs)):
+        ld, ad = l.double(), m.cuda().double()
+        assert (torch.linalg.norm(ld @ ld.T - ad) / torch.linalg.norm(ad)).item() <= 1e-5
