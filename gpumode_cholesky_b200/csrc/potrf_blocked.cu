@@ -454,6 +454,7 @@ struct TrailStream {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
   cudaEvent_t join = nullptr;
+  int priority = 0;  // the device's greatest (numerically lowest) launch priority
 };
 constexpr int kTrailDevices = 64;
 TrailStream g_trail[kTrailDevices];
@@ -469,10 +470,35 @@ int trail_stream(TrailStream** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t.join, cudaEventDisableTiming);
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "trail stream set-up: %s", cudaGetErrorString(e));
+    t.priority = greatest;
   }
   *out = &t;
   return B2P_OK;
+}
+
+// Launches `k` on `s`.  With `prio` set its CTAs take that launch priority,
+// so they go first when the look-ahead's side-stream update holds the SMs
+// (a CUDA graph's kernel node keeps the priority too).
+template <typename... KArgs, typename... Args>
+int launch_prio(const char* what, void (*k)(KArgs...), dim3 grid, int threads, size_t smem, cudaStream_t s,
+                const int* prio, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3((unsigned)threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (prio != nullptr) {
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = *prio;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k, args...);
+  return e == cudaSuccess ? B2P_OK : set_error(B2P_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 }  // namespace
 
@@ -500,6 +526,14 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
   // factor a 256-wide block column (their trailing updates limited to its
   // columns); one tcgen05 SYRK with K = 256 then updates the rest.
   const int outer = (tensor && n >= kTwoLevelMin) ? kOuterNB : n;
+  // FP32 look-ahead: diag, panel and the next column's update carry the
+  // critical path, so they launch at the device's greatest priority.
+  const int* prio = nullptr;
+  if (!tensor && n > kNB) {
+    TrailStream* ts0 = nullptr;
+    if (int st = trail_stream(&ts0)) return st;
+    prio = &ts0->priority;
+  }
   for (int K0 = 0; K0 < n; K0 += outer) {
     const int jmax = std::min(n, K0 + outer);
     for (int k0 = K0; k0 < jmax; k0 += kNB) {
@@ -507,12 +541,12 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       const int dgrid = (int)std::min<int64_t>(batch, (int64_t)sms * 16);
       {
         TraceScope ts(kKDiag, s);
-        if (f64diag)
-          diag_kernel_f64<<<dgrid, kD64Threads, kDiagF64Smem, s>>>(src, l, sch, k0, tws, info);
-        else
-          diag_kernel<false><<<dgrid, kD64Threads, dsmem, s>>>(src, l, sch, k0, tws, info);
+        const int st = f64diag ? launch_prio("diag_kernel_f64", diag_kernel_f64, dim3(dgrid), kD64Threads,
+                                             kDiagF64Smem, s, prio, src, l, sch, k0, tws, info)
+                               : launch_prio("diag_kernel", diag_kernel<false>, dim3(dgrid), kD64Threads, dsmem, s,
+                                             prio, src, l, sch, k0, tws, info);
+        if (st) return st;
       }
-      if (int st = check_launch("diag_kernel")) return st;
       const int R = n - k0 - kNB;
       if (R <= 0) {
         // The FP32 look-ahead's stream rejoins the caller's before the end.
@@ -527,9 +561,10 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       const int T = (R + kTile - 1) / kTile;
       {
         TraceScope ts(kKPanel, s);
-        panel_kernel<false><<<dim3(T, gy), kTrailThreads, 0, s>>>(src, l, sch, k0, tws);
+        if (int st = launch_prio("panel_kernel", panel_kernel<false>, dim3(T, gy), kTrailThreads, 0, s, prio, src, l,
+                                 sch, k0, tws))
+          return st;
       }
-      if (int st = check_launch("panel_kernel")) return st;
       if (k0 + kNB >= jmax) continue;
       if (tensor) {
         if (int st = launch_syrk_tc(src, l, sch, false, T_tc(n, k0), k0, mode, info, s, jmax < n ? jmax : 0))
@@ -549,9 +584,10 @@ int potrf_blocked(const float* a, float* l, int64_t batch, int n, int mode, void
       }
       {
         TraceScope ts(kKTrail, s);
-        trail_kernel<false><<<dim3(T, gy), kTrailThreads, tsmem, s>>>(src, l, sch, k0, 1);
+        if (int st = launch_prio("trail_kernel", trail_kernel<false>, dim3(T, gy), kTrailThreads, tsmem, s, prio, src,
+                                 l, sch, k0, 1))
+          return st;
       }
-      if (int st = check_launch("trail_kernel")) return st;
       if (int st = check(cudaEventRecord(ts2->fork, s), "cudaEventRecord")) return st;
       if (int st = check(cudaStreamWaitEvent(ts2->stream, ts2->fork, 0), "cudaStreamWaitEvent")) return st;
       if (T > 1) {
