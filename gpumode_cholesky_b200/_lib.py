@@ -59,6 +59,11 @@ SIGNATURES = {
         ctypes.c_int,
         [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
     ),
+    "b2p_potrf_host_workspace_size": (_c_sz, [_c_i64, _c_i64, ctypes.c_int, _c_i64]),
+    "b2p_potrf_batched_host": (
+        ctypes.c_int,
+        [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_i64, _c_p, _c_sz, _c_p, _c_p],
+    ),
     "b2p_noalloc_scratch_bytes": (_c_sz, []),
     "b2p_potrf_batched_noalloc": (ctypes.c_int, [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_ragged_plan_create": (ctypes.c_int, [_c_p, _c_p, _c_i64, ctypes.c_int, ctypes.c_int, _c_p]),

@@ -111,6 +111,62 @@ def cholesky(
     return out
 
 
+def cholesky_host(
+    a: torch.Tensor,
+    mode: str | int | None = None,
+    out: torch.Tensor | None = None,
+    info: torch.Tensor | None = None,
+    chunk: int = 0,
+    non_blocking: bool = False,
+) -> torch.Tensor:
+    """Factor a batch held in host memory into host memory on the current GPU.
+
+    The batch streams through the device in chunks of ``chunk`` matrices
+    (0: about 32 MiB each, at least four): the copy in of the next chunk, the
+    factorization of this one and the copy out of the previous one overlap
+    (``b2p_potrf_batched_host``).  ``a`` and ``out`` should be pinned
+    (``pin_memory()``) for the copies to overlap; ``out`` defaults to a new
+    pinned tensor.  ``info`` is an optional int32 CUDA tensor as for
+    :func:`cholesky`.  With ``non_blocking`` the call only enqueues, like
+    ``Tensor.copy_(..., non_blocking=True)``: ``out`` holds L once the
+    current stream is synchronised, and ``a`` and ``out`` must be kept
+    alive until then.
+    """
+    if not isinstance(a, torch.Tensor):
+        raise TypeError("input must be a torch.Tensor")
+    if a.dim() != 3 or a.shape[-1] != a.shape[-2]:
+        raise ValueError(f"input must have shape (batch, n, n), got {tuple(a.shape)}")
+    if a.dtype != torch.float32:
+        raise TypeError(f"input dtype must be torch.float32, got {a.dtype}")
+    if a.is_cuda:
+        raise ValueError("cholesky_host takes a host tensor; use cholesky() for a CUDA tensor")
+    if chunk < 0:
+        raise ValueError("chunk must be >= 0")
+    a = a.contiguous()
+    batch, n, _ = a.shape
+    code = resolve_mode(mode, n)
+    if out is None:
+        out = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+    elif out.shape != a.shape or out.dtype != torch.float32 or not out.is_contiguous() or out.is_cuda:
+        raise ValueError("out must be a contiguous float32 host tensor shaped like the input")
+    device = torch.device("cuda", torch.cuda.current_device())
+    info_ptr = None
+    if info is not None:
+        if info.dtype != torch.int32 or info.numel() < batch or not info.is_cuda:
+            raise ValueError("info must be an int32 CUDA tensor with at least batch elements")
+        info_ptr = info.data_ptr()
+    lib = _lib.load()
+    ws_bytes = lib.b2p_potrf_host_workspace_size(batch, n, code, chunk)
+    ws_ptr = workspace(device, ws_bytes).data_ptr() if ws_bytes else None
+    st = lib.b2p_potrf_batched_host(
+        a.data_ptr(), out.data_ptr(), batch, n, code, chunk, ws_ptr, ws_bytes, info_ptr, _stream_ptr(device)
+    )
+    _lib.check(st, "b2p_potrf_batched_host")
+    if not non_blocking:
+        torch.cuda.current_stream(device).synchronize()
+    return out
+
+
 def custom_kernel(data: torch.Tensor) -> torch.Tensor:
     """Drop-in for the reference entry point ``custom_kernel`` (submission.py:4101).
 

@@ -2,13 +2,15 @@
  * b200_potrf.h -- C ABI of the B200 batched Cholesky (potrf) library.
  *
  * The library factors SPD matrices A = L L^T on an NVIDIA B200 (sm_100a).
- * All buffers are device pointers owned by the caller; the library allocates
- * nothing on its own and keeps no state between calls except read-only
- * tables.  Every entry point returns an int status (B2P_OK on success) and
- * never aborts; b2p_status_string() and b2p_last_error() describe failures.
- * Work is enqueued on the caller's stream (a cudaStream_t passed as void*;
- * NULL means the legacy default stream) and nothing synchronises the host,
- * so every call can be captured in a CUDA graph.
+ * All buffers are device pointers owned by the caller (b2p_potrf_batched_host
+ * alone takes host matrices); the library allocates no device memory on its
+ * own and keeps no state between calls except read-only tables and its own
+ * streams and events.  Every entry point returns an int status (B2P_OK on
+ * success) and never aborts; b2p_status_string() and b2p_last_error()
+ * describe failures.  Work is enqueued on the caller's stream (a cudaStream_t
+ * passed as void*; NULL means the legacy default stream) and nothing
+ * synchronises the host, so every device-buffer call can be captured in a
+ * CUDA graph.
  *
  * Layout: a batch of `batch` matrices, each n x n, FP32, row-major and
  * contiguous (matrix b starts at element b*n*n).  The output holds L in the
@@ -114,6 +116,34 @@ B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n
 B2P_API size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int path);
 B2P_API int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
                                    void* workspace, size_t workspace_bytes, int32_t* info, void* stream);
+
+/*
+ * Host-resident batches: factors a (batch, n, n) FP32 batch held in HOST
+ * memory into host memory.  The batch streams through the current device in
+ * chunks of `chunk` matrices (0: the library's choice, about 32 MiB and at
+ * least four chunks).  The copy in of chunk i+1 (a library stream), the
+ * factorization of chunk i (b2p_potrf_batched on `stream`) and the copy out
+ * of chunk i-1 (a second library stream) overlap, so a call costs about one
+ * direction's PCIe transfer plus one chunk, not both directions in turn.
+ *   host_a, host_l  host pointers, batch*n*n floats each, not overlapping;
+ *              page-locked (cudaHostAlloc / cudaHostRegister) for the copies
+ *              to overlap (pageable memory works, one copy at a time).
+ *   workspace  device scratch of b2p_potrf_host_workspace_size() bytes,
+ *              256-byte aligned: two input and two output chunk buffers
+ *              plus the factorization's workspace for one chunk.
+ *   info       optional DEVICE int32[batch], as for b2p_potrf_batched.
+ * The call enqueues and returns: host_l holds L once `stream` has passed the
+ * call (cudaStreamSynchronize or an event), and host_a, host_l and the
+ * workspace must stay valid until then.  Every copy is ordered after the work
+ * already on `stream`, and `stream` waits for every copy before its next
+ * work.  Chunks use the same algorithm choice as b2p_potrf_batched for their
+ * own batch size.  No counterpart exists in the reference: its inputs are
+ * made on the device (reference/reference.py:37-55).
+ */
+B2P_API size_t b2p_potrf_host_workspace_size(int64_t batch, int64_t n, int mode, int64_t chunk);
+B2P_API int b2p_potrf_batched_host(const float* host_a, float* host_l, int64_t batch, int64_t n, int mode,
+                                   int64_t chunk, void* workspace, size_t workspace_bytes, int32_t* info,
+                                   void* stream);
 
 /*
  * Allocation-free variant of b2p_potrf_batched for callers that cannot

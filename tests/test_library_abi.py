@@ -65,6 +65,57 @@ def test_argument_validation_without_device():
     assert b"overlap" in lib.b2p_last_error()
 
 
+def test_host_entry_layout_and_validation_without_device():
+    """b2p_potrf_batched_host: chunk layout and the checks made before any CUDA call."""
+    lib = _lib.load()
+    bf = _lib.MODE_BF16X3
+    mib = 1 << 20
+    # One chunk (3 small matrices): one input and one output buffer, no factorization workspace.
+    assert lib.b2p_potrf_host_workspace_size(3, 16, 0, 0) == 2 * 3 * 16 * 16 * 4
+    # 640 x 512 by default: 32 MiB chunks of 32 matrices, two buffers per direction,
+    # plus the factorization's workspace for one chunk.
+    ws = lib.b2p_potrf_host_workspace_size(640, 512, bf, 0)
+    assert ws == 4 * 32 * mib + lib.b2p_potrf_workspace_size(32, 512, bf)
+    # An explicit chunk that does not divide the batch: the larger of the two chunk workspaces.
+    ws7 = lib.b2p_potrf_host_workspace_size(20, 256, bf, 7)
+    need = max(lib.b2p_potrf_workspace_size(7, 256, bf), lib.b2p_potrf_workspace_size(6, 256, bf))
+    assert ws7 == 4 * 7 * 256 * 256 * 4 + (need + 255) // 256 * 256
+    # A chunk at least the batch is one chunk.
+    assert lib.b2p_potrf_host_workspace_size(4, 64, 0, 100) == 2 * 4 * 64 * 64 * 4
+    assert lib.b2p_potrf_host_workspace_size(0, 64, 0, 0) == 0
+    assert lib.b2p_potrf_host_workspace_size(4, 64, 0, -1) == 0
+
+    host = ctypes.create_string_buffer(2 * 4 * 64 * 64 * 4 + 512)
+    base = (ctypes.addressof(host) + 255) // 256 * 256
+    a, l = ctypes.c_void_p(base), ctypes.c_void_p(base + 4 * 64 * 64 * 4)
+    call = lib.b2p_potrf_batched_host
+    assert call(None, None, 0, 64, 0, 0, None, 0, None, None) == _lib.B2P_OK
+    assert call(a, l, 4, 64, 0, -2, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert call(a, l, 4, 64, 0x77, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert call(None, l, 4, 64, 0, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert call(a, ctypes.c_void_p(base + 64), 4, 64, 0, 0, None, 0, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert b"overlap" in lib.b2p_last_error()
+    assert call(a, l, 4, 64, 0, 0, None, 0, None, None) == _lib.B2P_ERR_WORKSPACE
+    assert str(2 * 4 * 64 * 64 * 4).encode() in lib.b2p_last_error()
+    assert call(a, l, 4, 64, 0, 0, ctypes.c_void_p(base + 16), 1 << 20, None, None) == _lib.B2P_ERR_INVALID_ARG
+    assert b"256-byte" in lib.b2p_last_error()
+
+
+def test_cholesky_host_rejects_device_and_bad_arguments():
+    import torch
+
+    from gpumode_cholesky_b200 import cholesky_host
+
+    with pytest.raises(TypeError):
+        cholesky_host(torch.zeros(2, 8, 8, dtype=torch.float64))
+    with pytest.raises(ValueError):
+        cholesky_host(torch.zeros(2, 8, 7))
+    with pytest.raises(ValueError):
+        cholesky_host(torch.zeros(2, 8, 8), chunk=-1)
+    with pytest.raises(ValueError):
+        cholesky_host(torch.zeros(2, 8, 8), out=torch.zeros(2, 8, 8, dtype=torch.float64))
+
+
 def test_workspace_sizes_are_host_only():
     lib = _lib.load()
     assert lib.b2p_potrf_workspace_size(4096, 32, 0) == 0
