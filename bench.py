@@ -846,6 +846,30 @@ def run_ours(args) -> int:
             # host result may differ from the device call's in the last bits.
             "max_abs_diff_vs_device": max(float((ho.to(o.device) - o).abs().max()) for ho, o in zip(host_out, outs[0])),
         }
+        # The copy floor: the same bytes in both directions at once (two
+        # streams), the least any host-to-host call can take over this link.
+        dev_in = [torch.empty_like(a) for a in sets[0]]
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+        def copies():
+            cur = torch.cuda.current_stream()
+            s_in.wait_stream(cur)
+            s_out.wait_stream(cur)
+            with torch.cuda.stream(s_in):
+                for hi, di in zip(host_in, dev_in):
+                    di.copy_(hi, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                for do, ho in zip(outs[0], host_out):
+                    ho.copy_(do, non_blocking=True)
+            cur.wait_stream(s_in)
+            cur.wait_stream(s_out)
+
+        copies()
+        torch.cuda.synchronize()
+        floor_ms = _timed(copies, 3)
+        e2e["copy_floor_us"] = round(floor_ms * 1000, 1)
+        e2e["frac_of_copy_floor"] = round(floor_ms / e2e_ms, 4)
+        del dev_in
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu and not args.quick:
