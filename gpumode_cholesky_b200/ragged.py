@@ -144,6 +144,130 @@ class RaggedPlan:
         return g
 
 
+def split_runs(orders: Sequence[int], offsets: Sequence[int], parts: int) -> list[tuple[int, int]]:
+    """Cut a packed list into at most ``parts`` contiguous runs of about equal bytes.
+
+    Returns (first, end) matrix indices of each non-empty run, in order.  A
+    run ends at the first matrix whose end reaches its share of the buffer.
+    """
+    count = len(orders)
+    if count == 0:
+        return []
+    parts = max(1, min(int(parts), count))
+    ends = [o + n * n for n, o in zip(orders, offsets)]
+    base, total = offsets[0], ends[-1]
+    runs, first = [], 0
+    for k in range(1, parts + 1):
+        target = base + (total - base) * k / parts
+        end = first
+        while end < count and (end == first or ends[end - 1] < target):
+            end += 1
+        if k == parts:
+            end = count
+        if end > first:
+            runs.append((first, end))
+            first = end
+        if first >= count:
+            break
+    return runs
+
+
+class RaggedHostPlan:
+    """Factor a packed ragged list held in host memory into host memory.
+
+    The list is cut into ``parts`` contiguous runs of about equal bytes
+    (:func:`split_runs`; 0 picks runs of about 160 MiB, at most 64), each
+    with its own :class:`RaggedPlan` (``plan_options`` are passed on).
+    :meth:`factor` copies run i in on a copy stream, factors it on the
+    current stream once it has arrived, and copies it out on a second copy
+    stream, so the copies of the runs before and after overlap its
+    factorization; PCIe is full duplex, so a call costs about one direction's
+    transfer plus one run.  The plan keeps full-size device buffers for the
+    input and the factors (each run has its own slice, so no buffer is
+    reused within a call).  Host buffers should be pinned for the copies to
+    overlap.  A run picks its dense groups from its own matrices, so results
+    can differ in the last bits from one plan over the whole list.
+    """
+
+    def __init__(
+        self,
+        orders: Sequence[int],
+        offsets: Sequence[int] | None = None,
+        mode: str | int | None = None,
+        parts: int = 0,
+        device: torch.device | str | None = None,
+        **plan_options,
+    ):
+        self.orders = [int(n) for n in orders]
+        self.offsets = [int(o) for o in (offsets if offsets is not None else pack_offsets(self.orders)[:-1])]
+        if len(self.offsets) != len(self.orders):
+            raise ValueError("orders and offsets differ in length")
+        if parts < 0:
+            raise ValueError("parts must be >= 0")
+        for i in range(1, len(self.orders)):
+            if self.offsets[i] < self.offsets[i - 1] + self.orders[i - 1] ** 2:
+                raise ValueError("a host plan needs ascending, non-overlapping offsets")
+        self.count = len(self.orders)
+        self.mode = resolve_mode(mode, max(self.orders, default=0))
+        self.total = max((o + n * n for n, o in zip(self.orders, self.offsets)), default=0)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if parts == 0:
+            parts = min(64, max(1, -(-self.total * 4 // (160 << 20))))
+        self.runs = []  # (first, end, element start, element end, plan)
+        for i0, i1 in split_runs(self.orders, self.offsets, parts):
+            e0 = self.offsets[i0]
+            e1 = self.offsets[i1 - 1] + self.orders[i1 - 1] ** 2
+            plan = RaggedPlan(
+                self.orders[i0:i1], [o - e0 for o in self.offsets[i0:i1]], self.mode, device=self.device, **plan_options
+            )
+            self.runs.append((i0, i1, e0, e1, plan))
+        self.dev_in = torch.empty(max(self.total, 1), dtype=torch.float32, device=self.device)
+        self.dev_out = torch.empty_like(self.dev_in)
+        self._s_in = torch.cuda.Stream(self.device)
+        self._s_out = torch.cuda.Stream(self.device)
+
+    def factor(
+        self,
+        a: torch.Tensor,
+        out: torch.Tensor | None = None,
+        info: torch.Tensor | None = None,
+        non_blocking: bool = False,
+    ) -> torch.Tensor:
+        """Factor every matrix of the host buffer ``a`` into ``out`` (same layout, host).
+
+        With ``non_blocking`` the call only enqueues: ``out`` holds the
+        factors once the current stream is synchronised.
+        """
+        if a.is_cuda or a.dtype != torch.float32 or a.dim() != 1:
+            raise ValueError("a must be a 1-D float32 host buffer")
+        if a.numel() < self.total:
+            raise ValueError(f"buffer holds {a.numel()} elements, the plan needs {self.total}")
+        if out is None:
+            out = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        elif out.is_cuda or out.dtype != torch.float32 or out.shape != a.shape:
+            raise ValueError("out must be a float32 host buffer shaped like a")
+        if info is not None and (info.dtype != torch.int32 or info.numel() < self.count or not info.is_cuda):
+            raise ValueError("info must be an int32 CUDA tensor with one entry per matrix")
+        with torch.cuda.device(self.device):
+            cur = torch.cuda.current_stream(self.device)
+            # Copies start after the work already on the caller's stream
+            # (an earlier call may still read the device buffers).
+            self._s_in.wait_stream(cur)
+            self._s_out.wait_stream(cur)
+            for i0, i1, e0, e1, plan in self.runs:
+                with torch.cuda.stream(self._s_in):
+                    self.dev_in[e0:e1].copy_(a[e0:e1], non_blocking=True)
+                cur.wait_stream(self._s_in)
+                plan.factor(self.dev_in[e0:e1], self.dev_out[e0:e1], info[i0:i1] if info is not None else None)
+                self._s_out.wait_stream(cur)
+                with torch.cuda.stream(self._s_out):
+                    out[e0:e1].copy_(self.dev_out[e0:e1], non_blocking=True)
+            cur.wait_stream(self._s_out)
+            if not non_blocking:
+                cur.synchronize()
+        return out
+
+
 #: Candidate plan options for :func:`autotune`: padded-order step for orders
 #: <= 1024 and above, path of the groups above 1024, and concurrent streams.
 AUTOTUNE_GRID: tuple[dict, ...] = tuple(

@@ -196,3 +196,38 @@ def test_autotune_picks_a_working_plan():
     for m, l in zip(mats, unpack(out, orders, offs)):
         ld, ad = l.double(), m.cuda().double()
         assert (torch.linalg.norm(ld @ ld.T - ad) / torch.linalg.norm(ad)).item() <= 1e-5
+
+
+def test_host_plan_runs_match_device_plans():
+    """RaggedHostPlan: host in, host out; each run equals its own device plan bit for bit."""
+    from gpumode_cholesky_b200.ragged import RaggedHostPlan
+
+    rng = np.random.default_rng(11)
+    orders = [int(x) for x in np.exp(rng.uniform(np.log(16), np.log(700), 120)).astype(int)]
+    mats = [inputs.well_conditioned(1, n, seed=n + 3 * i, device="cpu")[0] for i, n in enumerate(orders)]
+    bad = 57
+    mats[bad] = -mats[bad]  # not SPD
+    host, orders, offs = pack(mats, device="cpu")
+    host = host.pin_memory()
+    plan = RaggedHostPlan(orders, offs, mode="bf16x3", parts=5)
+    assert len(plan.runs) == 5
+    info = torch.full((len(orders),), -4, dtype=torch.int32, device="cuda")
+    out = torch.zeros_like(host).pin_memory()
+    plan.factor(host, out, info=info, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    want = [int(oracle.potrf_f64(m.unsqueeze(0).numpy())[1][0]) for m in mats]
+    assert info.cpu().tolist() == want
+    dev = host.cuda()
+    for i0, i1, e0, e1, p in plan.runs:
+        ref = p.factor(dev[e0:e1]).cpu()
+        for n, o in zip(orders[i0:i1], offs[i0:i1]):
+            torch.testing.assert_close(out[o : o + n * n], ref[o - e0 : o - e0 + n * n], rtol=0, atol=0, equal_nan=True)
+    for i, (m, l) in enumerate(zip(mats, unpack(out, orders, offs))):
+        if i == bad:
+            continue
+        ld, ad = l.double(), m.double()
+        assert (torch.linalg.norm(ld @ ld.T - ad) / torch.linalg.norm(ad)).item() <= 1e-5, m.shape
+    # a blocking second call on pageable buffers gives the same factors
+    again = plan.factor(host.clone())
+    for x, y in zip(unpack(again, orders, offs), unpack(out, orders, offs)):
+        torch.testing.assert_close(x, y, rtol=0, atol=0, equal_nan=True)

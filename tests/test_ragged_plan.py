@@ -138,3 +138,36 @@ def test_plan_options():
     assert lib.b2p_ragged_plan_create_ex(offs, ns, 2, _lib.MODE_BF16X3, None, ctypes.byref(h)) == _lib.B2P_OK
     assert lib.b2p_ragged_plan_workspace_bytes(h) >= 2 * 4 * 320**2
     lib.b2p_ragged_plan_destroy(h)
+
+
+def test_split_runs_cover_the_list_in_order():
+    import random
+
+    from gpumode_cholesky_b200.ragged import split_runs
+
+    rng = random.Random(5)
+    for _ in range(300):
+        orders = [rng.choice([1, 3, 16, 64, 200, 1000, 2048]) for _ in range(rng.randint(1, 60))]
+        offs = inputs.pack_offsets(orders)[:-1]
+        parts = rng.randint(1, 70)
+        runs = split_runs(orders, offs, parts)
+        assert runs[0][0] == 0 and runs[-1][1] == len(orders)
+        assert all(a < b for a, b in runs)
+        assert all(runs[i][1] == runs[i + 1][0] for i in range(len(runs) - 1))
+        assert len(runs) <= min(parts, len(orders))
+    # equal orders split evenly
+    assert split_runs([10] * 8, inputs.pack_offsets([10] * 8)[:-1], 4) == [(0, 2), (2, 4), (4, 6), (6, 8)]
+    assert split_runs([], [], 3) == []
+
+
+def test_host_plan_rejects_overlapping_offsets():
+    import pytest
+
+    from gpumode_cholesky_b200.ragged import RaggedHostPlan
+
+    with pytest.raises(ValueError):
+        RaggedHostPlan([4, 4], [0, 8])  # the second matrix starts inside the first
+    with pytest.raises(ValueError):
+        RaggedHostPlan([4], [0, 16])
+    with pytest.raises(ValueError):
+        RaggedHostPlan([4, 4], parts=-1)
