@@ -761,6 +761,7 @@ def run_ours(args) -> int:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     from gpumode_cholesky_b200 import _lib, build
+    from gpumode_cholesky_b200 import checker
     from gpumode_cholesky_b200.potrf import cholesky, cholesky_host
 
     if not build.LIB_PATH.exists():
@@ -837,18 +838,19 @@ def run_ours(args) -> int:
             * _timed(lambda: [torch.linalg.cholesky_ex(a, check_errors=False) for a in sets[0]], max(2, args.steps // 2)),
             1,
         )
-        # Accuracy at full size (FP64 on the device).
+        # Accuracy at full size on the device: the relative Frobenius residual
+        # in FP64, and the reference checker's verdict (FP32 reconstruction).
         eager_step(0)
-        resid = {}
+        resid, verdicts = {}, {}
         for (b, n), a, o in zip(shapes, sets[0], outs[0]):
-            ld, ad = o.double(), a.double()
-            r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - ad) / torch.linalg.matrix_norm(ad)
-            resid[f"{b}x{n}"] = float(r.max())
+            resid[f"{b}x{n}"] = float(checker.residual_norms(a, o, precision="fp64")["rel_fro"].max())
+            verdicts[f"{b}x{n}"] = checker.check(a, o)[1]
         extra = {
             "per_shape_us": per_shape,
             "plain_fp32_us": plain,
             "cusolver_same_gpu_us": cus,
             "rel_residual_fro": resid,
+            "reference_checker": verdicts,
         }
 
     # Per-kernel device time of one eager step (CUDA events on the launch stream).
