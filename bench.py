@@ -62,7 +62,7 @@ WORKLOADS = {
         "sets": 8,
         "desc": "small batched potrf: 4096x32 FP32, MM^T/n+I",
         "metric": "batched potrf us per step (4096x32)",
-        # the shipped kernel's device time for this exact shape
+        # the reference's published device time of its shipped kernel for this exact shape
         "baseline_us": 14.0,
     },
     "ragged": {
