@@ -8,13 +8,14 @@ behind a C ABI (``include/b200_potrf.h``), called from Python through ctypes.
 from ._lib import LaunchTrace, PotrfError
 from .autograd import CholeskyFunction, cholesky_differentiable, potrf_backward
 from .gp import gp_nll, trsv
-from .potrf import cholesky, cholesky_host, custom_kernel
+from .potrf import cholesky, cholesky_checked, cholesky_host, custom_kernel
 
 __all__ = [
     "CholeskyFunction",
     "LaunchTrace",
     "PotrfError",
     "cholesky",
+    "cholesky_checked",
     "cholesky_host",
     "cholesky_differentiable",
     "custom_kernel",

@@ -167,6 +167,73 @@ def cholesky_host(
     return out
 
 
+def residual_estimate(a: torch.Tensor, l: torch.Tensor, probes: int = 4, seed: int = 0) -> torch.Tensor:
+    """Per-matrix estimate of ||L L^T - A||_F / ||A||_F from random probes, in FP64.
+
+    For V with ``probes`` N(0, 1) columns, E[||(L L^T - A) V||_F^2] equals
+    probes * ||L L^T - A||_F^2, so ||L (L^T V) - A V||_F / (sqrt(probes)
+    ||A||_F) estimates the relative residual at O(probes * n^2) per matrix
+    instead of the n^3 of forming L L^T.  A non-finite factor gives inf.
+    ``probes=0`` forms L L^T exactly in FP64 instead.
+    """
+    if probes == 0:
+        from .checker import residual_norms
+
+        return residual_norms(a, l, precision="fp64")["rel_fro"]
+    batch, n, _ = a.shape
+    gen = torch.Generator(device=a.device)
+    gen.manual_seed(seed)
+    out = torch.empty(batch, dtype=torch.float64, device=a.device)
+    step = max(1, (1 << 28) // max(1, n * n))  # slices of about 2 GiB of FP64 factor
+    for b0 in range(0, batch, step):
+        ld = l[b0 : b0 + step].double()
+        ad = a[b0 : b0 + step].double()
+        v = torch.randn((ld.shape[0], n, probes), dtype=torch.float64, device=a.device, generator=gen)
+        r = torch.matmul(ld, torch.matmul(ld.transpose(-1, -2), v)) - torch.matmul(ad, v)
+        est = torch.linalg.matrix_norm(r) / (probes**0.5 * torch.linalg.matrix_norm(ad).clamp_min(1e-300))
+        out[b0 : b0 + ld.shape[0]] = torch.where(torch.isfinite(est), est, torch.full_like(est, float("inf")))
+    return out
+
+
+def cholesky_checked(
+    a: torch.Tensor,
+    mode: str | int | None = "bf16x3",
+    tol: float = 1.0e-5,
+    probes: int = 4,
+    info: torch.Tensor | None = None,
+    out: torch.Tensor | None = None,
+) -> tuple[torch.Tensor, torch.Tensor]:
+    """Factor in ``mode``, then refactor in FP32 every matrix whose factor fails a residual check.
+
+    A matrix is refactored when its pivot check fails (``info`` != 0) or its
+    relative residual (:func:`residual_estimate`, ``probes`` random vectors;
+    0 for the exact FP64 check) exceeds ``tol`` or is not finite.  The
+    mixed modes keep their speed on the matrices they factor well, and
+    ill-conditioned ones fall back to the FP32 path of this library, not to
+    a CPU or vendor routine.  Returns (L, redone): ``redone`` is a bool CUDA
+    tensor marking the refactored matrices.  Synchronises the host once, to
+    learn whether any matrix needs the FP32 pass.
+    """
+    _check_input(a)
+    a = a.contiguous()
+    batch = a.shape[0]
+    own_info = torch.zeros(batch, dtype=torch.int32, device=a.device)
+    l = cholesky(a, mode=mode, out=out, info=own_info)
+    est = residual_estimate(a, l, probes=probes)
+    redone = (own_info != 0) | ~(est <= tol)
+    idx = redone.nonzero().flatten()
+    if idx.numel() > 0:
+        sub_info = torch.zeros(idx.numel(), dtype=torch.int32, device=a.device)
+        sub = cholesky(a.index_select(0, idx), mode="fp32", info=sub_info)
+        l.index_copy_(0, idx, sub)
+        own_info.index_copy_(0, idx, sub_info)
+    if info is not None:
+        if info.dtype != torch.int32 or info.numel() < batch or not info.is_cuda:
+            raise ValueError("info must be an int32 CUDA tensor with at least batch elements")
+        info[:batch].copy_(own_info)
+    return l, redone
+
+
 def custom_kernel(data: torch.Tensor) -> torch.Tensor:
     """Drop-in for the reference entry point ``custom_kernel`` (submission.py:4101).
 
