@@ -69,6 +69,7 @@ struct HostPipe {
 HostPipe g_pipe[kHostDevices];
 std::mutex g_pipe_mu;  // held while a call enqueues (the events are shared)
 
+// Caller holds g_pipe_mu.
 int host_pipe(HostPipe** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kHostDevices)
@@ -123,13 +124,13 @@ int b2p_potrf_batched_host(const float* host_a, float* host_l, int64_t batch, in
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", h.total, workspace_bytes);
   if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
     return set_error(B2P_ERR_INVALID_ARG, "workspace must be 256-byte aligned");
-  HostPipe* p = nullptr;
-  if (int st = host_pipe(&p)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   void* potrf_ws = h.potrf_bytes ? ws + h.potrf_off : nullptr;
 
-  std::lock_guard<std::mutex> lock(g_pipe_mu);
+  std::lock_guard<std::mutex> lock(g_pipe_mu);  // also guards the first call's stream set-up
+  HostPipe* p = nullptr;
+  if (int st = host_pipe(&p)) return st;
   // The copy streams start after the work already on the caller's stream
   // (it may still use the workspace or the host buffers).
   if (int st = check(cudaEventRecord(p->fork, s), "cudaEventRecord")) return st;
