@@ -253,8 +253,12 @@ def run_reference(args) -> int:
             oracle.ref_kernel_cpu(a)
     dt = (time.perf_counter() - t0) / args.steps
     scale = sum(_flops(b, n) for b, n in wl["shapes"]) / sum(_flops(b, n) for b, n in sample)
-    us = dt * 1e6 * scale
+    # With N GPUs every rank of the library's arm factors a full step, so the
+    # whole job is N steps' work; the host cores do that work in turn.
+    us = dt * 1e6 * scale * ws
     desc = " + ".join(f"{b}x{n}" for b, n in sample) + f" per step, scaled by flops x{scale:.2f} to the full step"
+    if ws > 1:
+        desc += f", x{ws} for the {ws} replicas of the whole job"
     line = {
         "impl": "reference",
         "metric": wl["metric"],
@@ -311,7 +315,7 @@ def _run_reference_ragged(args, wl, ws: int, threads: int) -> int:
         for m in mats:
             oracle.ref_kernel_cpu(m)
     dt = (time.perf_counter() - t0) / args.steps
-    us = dt * 1e6 * scale
+    us = dt * 1e6 * scale * ws  # the whole job: one draw per replica
     line = {
         "impl": "reference",
         "metric": wl["metric"],
@@ -333,7 +337,8 @@ def _run_reference_ragged(args, wl, ws: int, threads: int) -> int:
             "cores": threads,
             "kind": "reference",
             "sample": f"torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) per matrix on every 50th "
-            f"order of the draw ({len(mats)} matrices), scaled by sum n^3 x{scale:.1f}",
+            f"order of the draw ({len(mats)} matrices), scaled by sum n^3 x{scale:.1f}"
+            + (f", x{ws} for the {ws} replicas of the whole job" if ws > 1 else ""),
         },
         "e2e": {"value": round(us, 1), "unit": "us", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
