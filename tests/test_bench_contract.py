@@ -42,8 +42,8 @@ def test_reference_arm_gp_is_unavailable():
 
 def test_reference_arm_two_ranks_prints_once():
     cmd = [
-        sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
-        "--master-addr", "127.0.0.1", "--master-port", "29561",
+        sys.executable, "-m", "torch.distributed.run", "--standalone", "--local-addr", "127.0.0.1",
+        "--nnodes=1", "--nproc-per-node", "2",
         "bench.py", "--impl", "reference", "--gpus", "2", "--workload", "small", "--steps", "1", "--warmup", "3",
     ]
     out = _lines(cmd, timeout=300)
