@@ -101,6 +101,32 @@ def test_host_entry_layout_and_validation_without_device():
     assert b"256-byte" in lib.b2p_last_error()
 
 
+def test_host_workspace_matches_the_chunk_model():
+    """The host entry's workspace: 2 buffers per direction (1 for one chunk) + one chunk's factor workspace."""
+    import random
+
+    lib = _lib.load()
+    rng = random.Random(3)
+    mib = 1 << 20
+    for _ in range(300):
+        n = rng.choice([1, 8, 32, 33, 64, 100, 128, 129, 256, 512, 640, 1024, 2048])
+        batch = rng.randint(1, 3000)
+        mode = rng.choice([_lib.MODE_FP32, _lib.MODE_TF32, _lib.MODE_BF16X3])
+        chunk = rng.choice([0, 0, 1, 5, 64, 5000])
+        mat = n * n * 4
+        c = chunk
+        if c == 0:
+            c = max(1, max(4 * mib, min(32 * mib, batch * mat // 4)) // mat)
+        c = min(c, batch)
+        nchunks = -(-batch // c)
+        nbuf = 2 if nchunks > 1 else 1
+        buf = -(-c * mat // 256) * 256
+        last = batch - (nchunks - 1) * c
+        fw = max(lib.b2p_potrf_workspace_size(c, n, mode), lib.b2p_potrf_workspace_size(last, n, mode))
+        want = 2 * nbuf * buf + -(-fw // 256) * 256
+        assert lib.b2p_potrf_host_workspace_size(batch, n, mode, chunk) == want, (batch, n, mode, chunk)
+
+
 def test_cholesky_host_rejects_device_and_bad_arguments():
     import torch
 
