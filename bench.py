@@ -113,6 +113,7 @@ WORKLOADS = {
         "desc": "large potrf: 1x32768 FP32, GG^T/n+0.1I",
         "metric": "potrf us per step (1x32768)",
         "baseline_us": 22980.53,
+        "cpu_sample": [(1, 16384)],
     },
 }
 
@@ -226,6 +227,50 @@ def _resolve_mode(mode: str, n: int):
     return "bf16x3" if n > 128 else "fp32"
 
 
+def _shapes(wl: dict, args) -> list[tuple[int, int]]:
+    return [(max(1, int(round(b * args.scale))), n) for b, n in wl["shapes"]]
+
+
+def _dense_config(wl: dict, args, ws: int, shapes) -> dict:
+    """The workload's config, identical in both arms of the bench."""
+    return {
+        "workload": wl["desc"] + ("" if args.scale == 1.0 else f" (batch scaled x{args.scale})"),
+        "shapes": [f"{b}x{n}" for b, n in shapes],
+        "mode": args.mode,
+        "modes": {f"{b}x{n}": _resolve_mode(args.mode, n) for b, n in shapes},
+        "entry": "custom_kernel(A)" if args.mode == "auto" else f"cholesky(A, mode={args.mode!r})",
+        "l2": "inputs larger than L2 (rotating sets where one set is smaller); no flush",
+        "timing": "CUDA-graph replay of one step, CUDA events, max over ranks",
+        "parallelism": f"weak scaling, {ws} rank(s) each a full step",
+    }
+
+
+def _ragged_config(wl: dict, args, ws: int) -> dict:
+    return {
+        "workload": wl["desc"],
+        "mode": args.mode,
+        "l2": "inputs larger than L2 (5.2 GB packed); no flush",
+        "timing": "CUDA-graph replay of the whole ragged plan, CUDA events, max over ranks",
+        "parallelism": f"weak scaling, {ws} rank(s) each a full draw",
+    }
+
+
+def _cpu_sample(wl: dict, shapes, args) -> tuple[list[tuple[int, int]], float]:
+    """The shapes the CPU legs factor per step and the flops scale to the full step.
+
+    The whole step, unless ``--ref-sample`` asks for a fraction of each batch
+    or the workload names a smaller stand-in (1 x 32768 takes minutes per
+    factorization on the host, so its CPU legs factor 1 x 16384 and scale by
+    flops).
+    """
+    if args.ref_sample is not None:
+        sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in shapes]
+    else:
+        sample = list(wl.get("cpu_sample", shapes))
+    scale = sum(_flops(b, n) for b, n in shapes) / sum(_flops(b, n) for b, n in sample)
+    return sample, scale
+
+
 # ---------------------------------------------------------------------------
 def run_reference(args) -> int:
     """The reference's CPU route (torch.linalg.cholesky_ex FP32, reference/reference.py:129-130)."""
@@ -242,7 +287,8 @@ def run_reference(args) -> int:
     if wl.get("gp"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no Gaussian-process or backward path (forward factorization only)"}))
         return 0
-    sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+    shapes = _shapes(wl, args)
+    sample, scale = _cpu_sample(wl, shapes, args)
     data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for _ in range(args.warmup):
         for a in data:
@@ -252,11 +298,13 @@ def run_reference(args) -> int:
         for a in data:
             oracle.ref_kernel_cpu(a)
     dt = (time.perf_counter() - t0) / args.steps
-    scale = sum(_flops(b, n) for b, n in wl["shapes"]) / sum(_flops(b, n) for b, n in sample)
     # With N GPUs every rank of the library's arm factors a full step, so the
     # whole job is N steps' work; the host cores do that work in turn.
     us = dt * 1e6 * scale * ws
-    desc = " + ".join(f"{b}x{n}" for b, n in sample) + f" per step, scaled by flops x{scale:.2f} to the full step"
+    if scale == 1.0:
+        desc = "the whole step (" + " + ".join(f"{b}x{n}" for b, n in sample) + ") every step"
+    else:
+        desc = " + ".join(f"{b}x{n}" for b, n in sample) + f" per step, scaled by flops x{scale:.2f} to the full step"
     if ws > 1:
         desc += f", x{ws} for the {ws} replicas of the whole job"
     line = {
@@ -273,7 +321,7 @@ def run_reference(args) -> int:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": wl["desc"], "l2": "inputs larger than L2"},
+        "config": _dense_config(wl, args, ws, shapes),
         "cpu_baseline": {
             "value": round(us, 1),
             "unit": "us",
@@ -287,12 +335,12 @@ def run_reference(args) -> int:
     return 0
 
 
-def _ragged_cpu_sample(orders, offsets, host_buf=None):
-    """Every 50th matrix of the draw (from the packed host buffer when given,
-    else freshly generated with the same distribution)."""
+def _ragged_cpu_sample(orders, offsets, host_buf=None, every: int = 50):
+    """Every ``every``-th matrix of the draw (from the packed host buffer when
+    given, else freshly generated with the same distribution)."""
     from gpumode_cholesky_b200 import inputs
 
-    idx = list(range(0, len(orders), 50))
+    idx = list(range(0, len(orders), every))
     if host_buf is not None:
         mats = [host_buf[offsets[i] : offsets[i] + orders[i] ** 2].view(1, orders[i], orders[i]) for i in idx]
     else:
@@ -307,9 +355,10 @@ def _run_reference_ragged(args, wl, ws: int, threads: int) -> int:
     from gpumode_cholesky_b200 import inputs
 
     orders = inputs.ragged_orders(wl["count"], seed=wl["orders_seed"])
-    mats, scale = _ragged_cpu_sample(orders, None)
-    for m in mats:
-        oracle.ref_kernel_cpu(m)
+    mats, scale = _ragged_cpu_sample(orders, None, every=1)
+    for _ in range(args.warmup):
+        for m in mats:
+            oracle.ref_kernel_cpu(m)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         for m in mats:
@@ -330,14 +379,14 @@ def _run_reference_ragged(args, wl, ws: int, threads: int) -> int:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": wl["desc"], "l2": "inputs larger than L2"},
+        "config": _ragged_config(wl, args, ws),
         "cpu_baseline": {
             "value": round(us, 1),
             "unit": "us",
             "cores": threads,
             "kind": "reference",
-            "sample": f"torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) per matrix on every 50th "
-            f"order of the draw ({len(mats)} matrices), scaled by sum n^3 x{scale:.1f}"
+            "sample": f"torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) per matrix over the whole draw "
+            f"({len(mats)} matrices) every step"
             + (f", x{ws} for the {ws} replicas of the whole job" if ws > 1 else ""),
         },
         "e2e": {"value": round(us, 1), "unit": "us", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -552,14 +601,8 @@ def run_ours_ragged(args, wl) -> int:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {
-                "workload": wl["desc"],
-                "mode": args.mode,
-                "plan_options": {k: getattr(plan.options, k) for k, _ in plan.options._fields_},
-                "l2": "inputs larger than L2 (5.2 GB packed); no flush",
-                "timing": "CUDA-graph replay of the whole ragged plan, CUDA events, max over ranks",
-                "parallelism": f"weak scaling, {ws} rank(s) each a full draw",
-            },
+            "config": _ragged_config(wl, args, ws),
+            "plan_options": {k: getattr(plan.options, k) for k, _ in plan.options._fields_},
             **extra,
             "autotune": tuned,
             "matrices_per_s": round(ws * len(orders) / (ms / 1000.0), 1),
@@ -687,7 +730,7 @@ def run_ours_gp(args, wl) -> int:
         if rank == 0 and ws == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             torch.set_num_threads(threads)
-            sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+            sample, _ = _cpu_sample(wl, wl["shapes"], args)
             cpairs = [inputs.rbf_kernel_batch(b, n, seed=s, device="cpu") for (b, n), s in zip(sample, wl["seeds"])]
 
             def cpu_step():
@@ -868,7 +911,9 @@ def run_ours(args) -> int:
     # The dominant kernel's share of one traced step, applied to the timed
     # (graph-replayed) step time: its device time inside the timed region.
     share = dom_ms / max(sum(t for _, t in totals.values()), 1e-12)
-    roof = _roofline(args.workload, shapes, dom_name, ms * share, dom_count, modes, _measured_peaks())
+    roof = _roofline(
+        args.workload, shapes, dom_name, ms * share, dom_count, tr.units().get(dom_name, 0.0), modes, _measured_peaks()
+    )
     roof["share_of_step"] = round(share, 4)
 
     # End to end through the public API: pinned host in, host out, every step.
@@ -923,15 +968,7 @@ def run_ours(args) -> int:
             ),
             "dtype": "f32",
             "data": "synthetic",
-            "config": {
-                "workload": wl["desc"] + ("" if args.scale == 1.0 else f" (batch scaled x{args.scale})"),
-                "shapes": [f"{b}x{n}" for b, n in shapes],
-                "mode": args.mode,
-                "modes": dict(zip([f"{b}x{n}" for b, n in shapes], modes)),
-                "l2": "inputs larger than L2 (rotating sets where one set is smaller); no flush",
-                "timing": "CUDA-graph replay of one step, CUDA events, max over ranks",
-                "parallelism": f"weak scaling, {ws} rank(s) each a full step",
-            },
+            "config": _dense_config(wl, args, ws, shapes),
             **extra,
             "matrices_per_s": round(ws * sum(b for b, _ in shapes) / (ms / 1000.0), 1),
             "gflops_per_s": round(ws * sum(_flops(b, n) for b, n in shapes) / (ms / 1000.0) / 1e9, 1),
@@ -952,18 +989,22 @@ def run_ours(args) -> int:
     return 0
 
 
-def _roofline(workload: str, shapes, name: str, ms: float, count: int, modes, peaks: dict) -> dict:
+def _roofline(workload: str, shapes, name: str, ms: float, count: int, units: float, modes, peaks: dict) -> dict:
     """Roofline of the dominant kernel over one step.
 
-    Algorithmic units: HBM-bound kernels (the n <= 32 warp kernel) count 8*n^2
-    bytes per matrix (read A, write L once); factorization kernels count the
-    flops B*n^3/3 of the matrices they factor (the fused and CTA kernels) or,
-    for the trailing-update kernels of the blocked path, the flops of the
-    lower triangle they update, R(R+1)*64 per matrix and step.
+    ``units`` is the algorithmic work the library attached to that kernel's
+    launches in one traced step (the launch trace): 8*n^2 bytes per matrix
+    for the HBM-bound n <= 32 warp kernel (read A, write L once), and for the
+    factorization kernels the flops B*n^3/3 of the matrices those launches
+    factor -- only theirs: a batch the dispatcher splits between two kernels
+    credits each with its own matrices.  Update kernels carry the flops of
+    their product.  Where a kernel carries none (the blocked FP32 path), its
+    trailing update counts the lower triangle it updates, R(R+1)*64 per
+    matrix and step.
     """
     traffic_tab = _profiled_traffic()
     if name == "potrf_warp32_kernel":
-        byts = sum(8.0 * b * n * n for b, n in shapes)
+        byts = units if units > 0 else sum(8.0 * b * n * n for b, n in shapes)
         achieved = byts / (ms / count / 1000.0) / 1e9
         tpu = traffic_tab.get((name, workload, "fp32"))
         return {
@@ -979,7 +1020,9 @@ def _roofline(workload: str, shapes, name: str, ms: float, count: int, modes, pe
             "launches": count,
             "ms": round(ms, 4),
         }
-    if name.startswith("trail"):
+    if units > 0:
+        flops = units
+    elif name.startswith("trail"):
         flops = 0.0
         for b, n in shapes:
             for k0 in range(0, n, 64):
@@ -1013,25 +1056,25 @@ def _cpu_baseline(args, wl) -> dict:
 
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    sample = [(max(1, int(round(b * args.ref_sample))), n) for b, n in wl["shapes"]]
+    shapes = _shapes(wl, args)
+    sample, scale = _cpu_sample(wl, shapes, args)
     data = [_make(wl["gen"], b, n, s, "cpu") for (b, n), s in zip(sample, wl["seeds"])]
     for a in data:
         oracle.ref_kernel_cpu(a)
-    reps = 2
+    reps = 3
     t0 = time.perf_counter()
     for _ in range(reps):
         for a in data:
             oracle.ref_kernel_cpu(a)
     dt = (time.perf_counter() - t0) / reps
-    scale = sum(_flops(b, n) for b, n in wl["shapes"]) / sum(_flops(b, n) for b, n in sample)
+    what = " + ".join(f"{b}x{n}" for b, n in sample)
     return {
         "value": round(dt * 1e6 * scale, 1),
         "unit": "us",
         "cores": threads,
         "kind": "reference",
         "sample": "torch.linalg.cholesky_ex FP32 on CPU (reference ref_kernel) on "
-        + " + ".join(f"{b}x{n}" for b, n in sample)
-        + f", scaled by flops x{scale:.2f}",
+        + (f"the whole step ({what}), mean of {reps}" if scale == 1.0 else f"{what}, scaled by flops x{scale:.2f}"),
     }
 
 
@@ -1043,7 +1086,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mid")
     ap.add_argument("--mode", default="auto")
-    ap.add_argument("--ref-sample", type=float, default=0.05, help="fraction of the step the CPU legs factor")
+    ap.add_argument(
+        "--ref-sample", type=float, default=None, help="fraction of each batch the CPU legs factor (default: all)"
+    )
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true", help="timed region and roofline only (for profiling)")
     ap.add_argument("--scale", type=float, default=1.0, help="batch scale (small profiling cases); 1 = the workload")

@@ -81,6 +81,7 @@ SIGNATURES = {
     "b2p_debug_tc_gemm": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_p]),
     "b2p_trace_enable": (ctypes.c_int, [ctypes.c_int]),
     "b2p_trace_read": (ctypes.c_int, [_c_p, _c_p, ctypes.c_int]),
+    "b2p_trace_read_units": (ctypes.c_int, [_c_p, ctypes.c_int]),
     "b2p_kernel_name": (ctypes.c_char_p, [ctypes.c_int]),
 }
 
@@ -125,12 +126,15 @@ class LaunchTrace:
     """Context manager recording per-launch device time of every library kernel.
 
     Use outside CUDA-graph capture.  ``records()`` returns (kernel name, ms)
-    pairs in launch order after synchronising the recorded events.
+    pairs in launch order after synchronising the recorded events;
+    ``units()`` the algorithmic work the library attached to each launch
+    (flops, or bytes for the n <= 32 kernel; 0 where none is defined).
     """
 
     def __init__(self, capacity: int = 65536):
         self.capacity = capacity
         self._records: list[tuple[str, float]] = []
+        self._units: list[float] = []
 
     def __enter__(self):
         check(load().b2p_trace_enable(self.capacity), "b2p_trace_enable")
@@ -142,11 +146,21 @@ class LaunchTrace:
         ms = (ctypes.c_float * self.capacity)()
         k = lib.b2p_trace_read(ids, ms, self.capacity)
         self._records = [(lib.b2p_kernel_name(ids[i]).decode(), float(ms[i])) for i in range(k)]
+        units = (ctypes.c_double * self.capacity)()
+        ku = lib.b2p_trace_read_units(units, self.capacity)
+        self._units = [float(units[i]) for i in range(min(k, ku))]
         lib.b2p_trace_enable(0)
         return False
 
     def records(self) -> list[tuple[str, float]]:
         return list(self._records)
+
+    def units(self) -> dict[str, float]:
+        """Algorithmic work per kernel name, summed over its launches."""
+        out: dict[str, float] = {}
+        for (name, _), u in zip(self._records, self._units):
+            out[name] = out.get(name, 0.0) + u
+        return out
 
     def totals(self) -> dict[str, tuple[int, float]]:
         out: dict[str, tuple[int, float]] = {}

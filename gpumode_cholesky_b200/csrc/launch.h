@@ -134,10 +134,13 @@ enum KernelId {
 };
 
 // RAII bracket: records a start/end CUDA event pair around one launch on
-// stream `s` while the trace is enabled; a no-op otherwise.
+// stream `s` while the trace is enabled; a no-op otherwise.  `units` is the
+// launch's algorithmic work: n^3/3 flops per matrix for the kernels that
+// factor whole matrices, 8 n^2 bytes per matrix for the n <= 32 kernel, the
+// product's flops for update kernels; 0 where none is defined.
 class TraceScope {
  public:
-  TraceScope(int kernel_id, cudaStream_t s);
+  TraceScope(int kernel_id, cudaStream_t s, double units = 0.0);
   ~TraceScope();
 
  private:

@@ -311,7 +311,7 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const size_t smem = two ? kFSmemBytes : std::max<size_t>(kFSmemBytes, kFSmemOneCta);
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
-  TraceScope ts(kKFused, s);
+  TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
   if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
     potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);

@@ -494,7 +494,7 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  TraceScope ts(kKFusedWs, s);
+  TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
   const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;

@@ -12,9 +12,15 @@
 // loads this library holds until the process exits.
 //
 // Limits and sharing:
-//   * the scratch holds kNoAllocScratchBytes (16 MiB); a call whose blocked
-//     path needs more (batch * 16 KiB for n > 128) is rejected with
-//     B2P_ERR_WORKSPACE before anything is launched;
+//   * the scratch holds kNoAllocScratchBytes (16 MiB); a call whose path
+//     needs more workspace than that is rejected with B2P_ERR_WORKSPACE
+//     before anything is launched, and the message gives the largest batch
+//     of that order and mode that fits.  Per matrix of order n > 128 the
+//     need is 16 KiB in FP32 (the blocked path: 1024 matrices per call);
+//     the tensor modes at n a multiple of 64 keep the panels' operand
+//     copies, 8192 (n/64) (n/64 - 1) bytes (about 36 matrices of order 512,
+//     8 of order 1024), plus 512 n bytes of panel buffers above order 1024
+//     (no single matrix above order 2752 fits);
 //   * every call on a device shares the one array and leaves its contents
 //     behind; nothing in it has to start at zero (each block inverse is
 //     written before it is read), so no clearing is needed;
@@ -22,7 +28,14 @@
 //     threads) race on the array: serialise them on one stream;
 //   * the first call on each device looks up the array's device address with
 //     cudaGetSymbolAddress (a host-side query, no allocation); make that first
-//     call before any stream capture.
+//     call before any stream capture.  The first call that reaches the split
+//     path (tensor modes above order 1024) or the FP32 path with its
+//     look-ahead also creates that path's library-owned streams and events
+//     once per device, so warm each path up once outside capture and outside
+//     any region that must not touch the driver;
+//   * the address is cached per device ordinal: after cudaDeviceReset (or
+//     any other teardown of the device's primary context) it is stale, so
+//     such a process must not call this entry point again.
 #include <mutex>
 
 #include "launch.h"
@@ -67,12 +80,19 @@ size_t b2p_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
 int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, int64_t n, int mode,
                               int32_t* info, void* stream) {
   const size_t need = b2p_potrf_workspace_size(batch, n, mode);
-  if (need > kNoAllocScratchBytes)
+  if (need > kNoAllocScratchBytes) {
+    // Largest batch of this order and mode whose workspace fits (the
+    // workspace grows with the batch, so bisect on it).
+    int64_t lo = 0, hi = batch;
+    while (hi - lo > 1) {
+      const int64_t mid = lo + (hi - lo) / 2;
+      if (b2p_potrf_workspace_size(mid, n, mode) <= kNoAllocScratchBytes) lo = mid; else hi = mid;
+    }
     return set_error(B2P_ERR_WORKSPACE,
-                     "batch=%lld n=%lld needs %zu bytes of scratch; the allocation-free entry point "
-                     "holds %zu (at most %zu matrices of order > 128 per call)",
-                     (long long)batch, (long long)n, need, kNoAllocScratchBytes,
-                     kNoAllocScratchBytes / (64 * 64 * sizeof(float)));
+                     "batch=%lld n=%lld mode 0x%x needs %zu bytes of scratch; the allocation-free entry point "
+                     "holds %zu (at most %lld matrices of this order and mode per call)",
+                     (long long)batch, (long long)n, mode, need, kNoAllocScratchBytes, (long long)lo);
+  }
   void* scratch = nullptr;
   if (need > 0) {
     if (int st = noalloc_scratch(&scratch)) return st;

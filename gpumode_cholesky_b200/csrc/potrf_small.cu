@@ -147,7 +147,7 @@ int launch_warp32(const float* a, float* l, const MatrixList& ml, int32_t* info,
   const int64_t ctas = (ml.count + kWarp32Warps - 1) / kWarp32Warps;
   const int grid = (int)std::min<int64_t>(ctas, (int64_t)device_sms() * 8 * 16);
   {
-    TraceScope ts(kKWarp32, s);
+    TraceScope ts(kKWarp32, s, ml.ns ? 0.0 : 8.0 * (double)ml.count * ml.n * ml.n);
     potrf_warp32_kernel<<<grid, kWarp32Warps * 32, 0, s>>>(a, l, ml, info);
   }
   return check_launch("potrf_warp32_kernel");
@@ -159,7 +159,7 @@ int launch_cta128(const float* a, float* l, const MatrixList& ml, int32_t* info,
   if (int st = ensure_smem_attr((const void*)potrf_cta128_kernel, smem, kSlotCta128)) return st;
   const int grid = (int)std::min<int64_t>(ml.count, (int64_t)device_sms() * 2 * 64);
   {
-    TraceScope ts(kKCta128, s);
+    TraceScope ts(kKCta128, s, ml.ns ? 0.0 : (double)ml.count * ml.n * ml.n * ml.n / 3.0);
     potrf_cta128_kernel<<<grid, kCta128Threads, smem, s>>>(a, l, ml, info);
   }
   return check_launch("potrf_cta128_kernel");

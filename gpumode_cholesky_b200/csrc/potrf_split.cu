@@ -834,7 +834,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TraceScope ts(kKSplitUpdate, st);
+    TraceScope ts(kKSplitUpdate, st, 2.0 * 64 * 64 * (double)(c1 - c0) * batch * (n - 64 * k));
     const cudaError_t e = cudaLaunchKernelEx(&cfg, upd, base, mstride, ld, (const uint8_t*)copies, pout, n, k,
                                              c0, c1, segs, info);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_update_kernel: %s", cudaGetErrorString(e));
@@ -864,7 +864,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    TraceScope ts(kKSplitWide, side->wide);
+    TraceScope ts(kKSplitWide, side->wide, 2.0 * 64 * (double)c1 * cols * batch * (n - j0));
     const cudaError_t e = cudaLaunchKernelEx(&cfg, wdk, (const float*)(a + j0), n2, n, (const uint8_t*)copies,
                                              bw[J & 1], (int64_t)n * nbw, nbw, batch, n, j0, cols, 0, c1, segs, info);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_wide_kernel: %s", cudaGetErrorString(e));
@@ -904,7 +904,10 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       attr[0].val.priority = side->step_priority;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      TraceScope ts(kKSplitStep, s);
+      // Diagonal factor, panel solve and the newest panel's product.
+      const double rows = (double)(n - 64 * k - 64);
+      TraceScope ts(kKSplitStep, s,
+                    batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
       const cudaError_t e = cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }

@@ -9,6 +9,7 @@ namespace b2p {
 namespace {
 struct Entry {
   int id;
+  double units;
   cudaEvent_t start, end;
 };
 std::mutex g_mu;
@@ -34,12 +35,13 @@ void free_all() {
 }
 }  // namespace
 
-TraceScope::TraceScope(int kernel_id, cudaStream_t s) : slot_(-1), s_(s) {
+TraceScope::TraceScope(int kernel_id, cudaStream_t s, double units) : slot_(-1), s_(s) {
   if (g_capacity == 0) return;
   std::lock_guard<std::mutex> lock(g_mu);
   if (g_used >= g_capacity) return;
   Entry e;
   e.id = kernel_id;
+  e.units = units;
   if (cudaEventCreate(&e.start) != cudaSuccess) return;
   if (cudaEventCreate(&e.end) != cudaSuccess) {
     cudaEventDestroy(e.start);
@@ -80,6 +82,17 @@ int b2p_trace_read(int32_t* kernel_ids, float* ms, int max_entries) {
     if (cudaEventSynchronize(e.end) == cudaSuccess) cudaEventElapsedTime(&t, e.start, e.end);
     if (kernel_ids) kernel_ids[k] = e.id;
     if (ms) ms[k] = t;
+    ++k;
+  }
+  return k;
+}
+
+int b2p_trace_read_units(double* units, int max_entries) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  int k = 0;
+  for (auto& e : g_entries) {
+    if (k >= max_entries) break;
+    if (units) units[k] = e.units;
     ++k;
   }
   return k;

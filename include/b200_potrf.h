@@ -152,12 +152,19 @@ B2P_API int b2p_potrf_batched_host(const float* host_a, float* host_l, int64_t b
  * allocation after start-up).  It takes no workspace: the scratch of the
  * blocked path lives in a 16 MiB device array inside this library, held by
  * every GPU that loads it until the process exits
- * (b2p_noalloc_scratch_bytes() reports the size).  A call needing more
- * (batch * 16 KiB for n > 128, i.e. more than 1024 such matrices) is
- * rejected with B2P_ERR_WORKSPACE.  Calls share the array: calls that overlap
- * on the GPU race, so serialise them on one stream.  The first call on each
- * device looks the array's address up (cudaGetSymbolAddress); make it before
- * any stream capture.  No counterpart exists in the reference.
+ * (b2p_noalloc_scratch_bytes() reports the size).  A call whose workspace
+ * (b2p_potrf_workspace_size) exceeds it is rejected with B2P_ERR_WORKSPACE,
+ * and the message names the largest batch of that order and mode that fits.
+ * For orders > 128 that is 1024 matrices in FP32, but the tensor modes keep
+ * every panel's operand copy, 8192 (n/64) (n/64 - 1) bytes per matrix:
+ * about 36 matrices of order 512, 8 of order 1024, and no single matrix
+ * above order 2752.  Calls share the array: calls that overlap on
+ * the GPU race, so serialise them on one stream.  The first call on each
+ * device looks the array's address up (cudaGetSymbolAddress), and the first
+ * call reaching the split or FP32 look-ahead paths creates their streams
+ * and events; make those warm-up calls before any stream capture.  The
+ * address is cached per device: do not call this again after
+ * cudaDeviceReset.  No counterpart exists in the reference.
  */
 B2P_API size_t b2p_noalloc_scratch_bytes(void);
 B2P_API int b2p_potrf_batched_noalloc(const float* a, float* l, int64_t batch, int64_t n,
@@ -289,10 +296,17 @@ B2P_API int b2p_debug_tc_gemm(const float* a, const float* b, float* d, int64_t 
  *                               (0 stops recording and frees the events);
  *   b2p_trace_read(ids, ms, max) synchronises the recorded events and writes
  *                               kernel ids and durations; returns the count;
+ *   b2p_trace_read_units(u, max) the algorithmic work of each recorded
+ *                               launch, in the same order: n^3/3 flops per
+ *                               matrix for kernels that factor whole
+ *                               matrices, 8 n^2 bytes per matrix for the
+ *                               n <= 32 kernel, the product's flops for
+ *                               update kernels, 0 where none is defined;
  *   b2p_kernel_name(id)         the kernel's name.
  */
 B2P_API int b2p_trace_enable(int capacity);
 B2P_API int b2p_trace_read(int32_t* kernel_ids, float* ms, int max_entries);
+B2P_API int b2p_trace_read_units(double* units, int max_entries);
 B2P_API const char* b2p_kernel_name(int id);
 
 #ifdef __cplusplus

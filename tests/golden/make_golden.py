@@ -1,9 +1,8 @@
 """Generates the golden fixtures in this directory from the reference itself.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run where a checkout of the reference exists, naming its root:
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_golden.py
 
 For every case it calls the reference's own ``generate_input`` and
 ``check_implementation`` (reference/reference.py:37-188) and its entry point
@@ -26,7 +25,9 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+if "REFERENCE_ROOT" not in os.environ:
+    sys.exit("set REFERENCE_ROOT to the root of the reference checkout")
+REF = Path(os.environ["REFERENCE_ROOT"])
 
 # (batch, n, cond, seed, case): the reference's own test specs
 # (scripts/_gpu_runner.py:40-109) at reduced batch, plus edge orders.
