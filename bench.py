@@ -222,9 +222,10 @@ def _profiled_traffic() -> dict:
 
 
 def _resolve_mode(mode: str, n: int):
+    """The mode name a shape runs in ("auto": what custom_kernel picks)."""
     if mode != "auto":
         return mode
-    return "bf16x3" if n > 128 else "fp32"
+    return "bf16x3+guard" if n > 128 and n % 64 == 0 else "fp32"
 
 
 def _shapes(wl: dict, args) -> list[tuple[int, int]]:
@@ -810,7 +811,7 @@ def run_ours(args) -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     from gpumode_cholesky_b200 import _lib, build
     from gpumode_cholesky_b200 import checker
-    from gpumode_cholesky_b200.potrf import cholesky, cholesky_host
+    from gpumode_cholesky_b200.potrf import cholesky, cholesky_host, custom_kernel
 
     if not build.LIB_PATH.exists():
         build.build()
@@ -825,7 +826,17 @@ def run_ours(args) -> int:
     outs = [[torch.empty_like(a) for a in st] for st in sets]
     torch.cuda.synchronize()
 
+    drop_in = args.mode == "auto"
+
     def eager_step(i: int, mode_list=None):
+        # The headline step is the reference-facing entry itself: one
+        # custom_kernel(A) call per shape, each returning a fresh output (a
+        # graph-pool tensor under capture, kept in outs).
+        if mode_list is None and drop_in:
+            st = sets[i % len(sets)]
+            for j, a in enumerate(st):
+                outs[i % len(sets)][j] = custom_kernel(a)
+            return
         ml = mode_list or modes
         for a, o, m in zip(sets[i % len(sets)], outs[i % len(sets)], ml):
             cholesky(a, mode=m, out=o)
@@ -877,7 +888,8 @@ def run_ours(args) -> int:
         per_shape = {}
         for j, ((b, n), m) in enumerate(zip(shapes, modes)):
             a, o = sets[0][j], outs[0][j]
-            per_shape[f"{b}x{n}"] = round(1000 * _timed(lambda: cholesky(a, mode=m, out=o), args.steps), 1)
+            call = (lambda: custom_kernel(a)) if drop_in else (lambda: cholesky(a, mode=m, out=o))
+            per_shape[f"{b}x{n}"] = round(1000 * _timed(call, args.steps), 1)
         plain = None
         if any(m != "fp32" for m in modes):
             plain = round(1000 * _timed(lambda: eager_step(0, ["fp32"] * len(shapes)), args.steps), 1)

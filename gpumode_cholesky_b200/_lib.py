@@ -24,6 +24,8 @@ MODE_TF32 = 1
 MODE_BF16X3 = 2
 MODE_FP8 = 3
 FLAG_FP64_DIAG = 0x100
+FLAG_GUARD = 0x200
+FLAGS = {"fp64diag": FLAG_FP64_DIAG, "guard": FLAG_GUARD}
 
 MODES = {"fp32": MODE_FP32, "tf32": MODE_TF32, "bf16x3": MODE_BF16X3, "fp8": MODE_FP8}
 
@@ -58,6 +60,10 @@ SIGNATURES = {
     "b2p_potrf_batched_path": (
         ctypes.c_int,
         [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p],
+    ),
+    "b2p_potrf_batched_ex": (
+        ctypes.c_int,
+        [_c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, ctypes.c_int, _c_p, _c_sz, _c_p, _c_p, _c_p],
     ),
     "b2p_potrf_host_workspace_size": (_c_sz, [_c_i64, _c_i64, ctypes.c_int, _c_i64]),
     "b2p_potrf_batched_host": (

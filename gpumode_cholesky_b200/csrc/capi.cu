@@ -103,18 +103,18 @@ size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
 }
 
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
-               int32_t* info, cudaStream_t s) {
+               int32_t* info, cudaStream_t s, int32_t* fp32_from) {
   switch (path) {
-    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s);
-    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s);
-    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
+    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
+    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
     default: return potrf_blocked(a, l, batch, n, mode, ws, ws_bytes, info, s);
   }
 }
 
 static int check_mode(int mode) {
   const int m = mode & B2P_MODE_MASK;
-  if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG)) != 0)
+  if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG | B2P_FLAG_GUARD)) != 0)
     return set_error(B2P_ERR_INVALID_ARG, "unknown mode 0x%x", mode);
   return B2P_OK;
 }
@@ -159,6 +159,11 @@ int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mo
 
 int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
                            void* workspace, size_t workspace_bytes, int32_t* info, void* stream) {
+  return b2p_potrf_batched_ex(a, l, batch, n, mode, path, workspace, workspace_bytes, info, nullptr, stream);
+}
+
+int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
+                         void* workspace, size_t workspace_bytes, int32_t* info, int32_t* fp32_from, void* stream) {
   g_msg[0] = '\0';
   if (int st = check_mode(mode)) return st;
   if (path < B2P_PATH_AUTO || path > B2P_PATH_SPLIT) return set_error(B2P_ERR_INVALID_ARG, "unknown path %d", path);
@@ -172,6 +177,11 @@ int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, i
   const char* pl = reinterpret_cast<const char*>(l);
   if (pa < pl + bytes && pl < pa + bytes) return set_error(B2P_ERR_INVALID_ARG, "input and output overlap");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (fp32_from != nullptr) {
+    // -1 everywhere; the guarded kernels overwrite the matrices they touch.
+    const cudaError_t e = cudaMemsetAsync(fp32_from, 0xff, (size_t)batch * sizeof(int32_t), s);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(fp32_from): %s", cudaGetErrorString(e));
+  }
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
   const bool auto_path = path == B2P_PATH_AUTO;
@@ -186,14 +196,15 @@ int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, i
     const int64_t tail = batch % per;
     if (batch > per && tail > 0 && tail * 2 <= per && fused_ws_supported(tail, n, mode)) {
       const int64_t head = batch - tail;
-      if (int st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s)) return st;
+      if (int st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, fp32_from)) return st;
       const size_t moff = (size_t)head * (size_t)n * (size_t)n;
       const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
       return potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
-                            workspace_bytes - woff, info ? info + head : nullptr, s);
+                            workspace_bytes - woff, info ? info + head : nullptr, s,
+                            fp32_from ? fp32_from + head : nullptr);
     }
   }
-  return potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s);
+  return potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, fp32_from);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

@@ -1,0 +1,157 @@
+// Pivot guard of the mixed-precision modes (B2P_FLAG_GUARD).
+//
+// In the tensor modes the update of block column k, D = L[:, 0:k0] L[k-block,
+// 0:k0]^T, is accumulated on the tensor core from rounded operands, so every
+// entry of D carries an error of about
+//     delta(k) * sum_c L_jc^2  <=  delta(k) * A_jj,
+//     delta(k) = 2^-16 (BF16x3: the operand split hi + lo keeps 16 bits)
+//              | 2^-10 (TF32: 11-bit operands, product error 2^-10)
+//                + (MMAs accumulated so far) * 2^-23 (the accumulator does
+//                  not round to nearest: one FP32 ulp per accumulation step),
+// and the pivot d_j = A_jj - D_jj - (within the block) inherits it.  When
+// d_j is not well above that error its sign and size are noise: this is how
+// the mixed modes fail on matrices whose Schur complements sink to the level
+// of a jitter term (Gaussian-process kernels) while the plain FP32 path
+// factors them.
+//
+// The guard therefore checks, after the diagonal block of column k is
+// factored, every pivot against
+//     d_j = L_jj^2  >  kGuardMargin * delta(k) * A_jj
+// (non-finite or non-positive pivots fail too).  When one fails, the column's
+// update is recomputed in FP32 on the SIMT cores from the FP32 factor already
+// written (L[:, 0:k0] is final), the column is refactored from it, and every
+// later column of that matrix is computed the same way: after the first
+// failure the factorization continues as the plain FP32 method would.  The
+// reference's closest analogue is the accurate retry of its 256-order kernel,
+// triggered when a pivot falls under 1e-2 of the input's diagonal
+// (submission.py:866-868, 883-886, 1004-1031), which refactors the whole
+// matrix in FP32.
+#pragma once
+
+#include <stdint.h>
+
+#include "launch.h"
+
+namespace b2p {
+
+constexpr float kGuardMargin = 2.0f;
+constexpr int kGuardStageLd = 36;  // floats per staged row of the FP32 update
+constexpr int kGuardStageFloats = 64 * kGuardStageLd;
+
+// Pivot threshold (relative to A_jj) for block column k (k0 = 64 k) of a
+// mode; 0 disables the check (no update before column 0).
+template <int MODE>
+__device__ __forceinline__ float guard_tau(int k) {
+  if (k == 0) return 0.0f;
+  constexpr float kRep = MODE == B2P_MODE_TF32 ? 9.765625e-4f : 1.52587890625e-5f;  // 2^-10, 2^-16
+  constexpr float kSteps = MODE == B2P_MODE_TF32 ? 8.0f : 12.0f;                      // MMAs per 64-wide chunk
+  return kGuardMargin * (kRep + kSteps * (float)k * 1.1920928955078125e-7f);         // 2^-23
+}
+
+// True when some pivot of the factored diagonal block (dg_s: L_kk, row stride
+// ld, w valid rows) fails the threshold against A's diagonal (a_diag: the
+// element A[k0][k0], diagonal stride n + 1).  Called by one full warp.
+__device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, const float* a_diag, int64_t n, int w,
+                                                  float tau, int lane) {
+  bool fail = false;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int j = lane + 32 * h;
+    if (j < w) {
+      const float ljj = dg_s[j * ld + j];
+      const float d = ljj * ljj;
+      const float ajj = __ldg(a_diag + (size_t)j * (n + 1));
+      if (!(d > tau * ajj)) fail = true;  // also catches NaN and non-positive pivots
+    }
+  }
+  return __any_sync(0xffffffffu, fail);
+}
+
+// FP32 update of one row against 32 columns of block column k, computed on
+// the SIMT cores: d[q] = sum_{j < k0} L[row][j] * L[k0 + c0 + q][j] (in order
+// of increasing j, fused multiply-adds).  Collective over the NT threads
+// that call it (barrier functor `bar`): each passes its own row (-1 for
+// none; d is then 0) and c0 (0 or 32, uniform within a warp); `stage` holds
+// kGuardStageFloats floats of shared memory, free until the call returns.
+template <int NT, class Bar>
+__device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __restrict__ L, int64_t n, int k0,
+                                                 int64_t row, int c0, float* stage, int tid, Bar bar) {
+#pragma unroll
+  for (int q = 0; q < 32; ++q) d[q] = 0.0f;
+  for (int j0 = 0; j0 < k0; j0 += 32) {
+    bar();  // the previous chunk's stage has been read
+    for (int e = tid; e < 64 * 8; e += NT) {
+      const int c = e >> 3, q4 = e & 7;
+      *reinterpret_cast<float4*>(stage + c * kGuardStageLd + 4 * q4) =
+          *reinterpret_cast<const float4*>(L + (size_t)(k0 + c) * n + j0 + 4 * q4);
+    }
+    bar();
+    if (row >= 0) {
+      float x[32];
+      const float4* src = reinterpret_cast<const float4*>(L + (size_t)row * n + j0);
+#pragma unroll
+      for (int q4 = 0; q4 < 8; ++q4) {
+        const float4 v = src[q4];
+        x[4 * q4 + 0] = v.x;
+        x[4 * q4 + 1] = v.y;
+        x[4 * q4 + 2] = v.z;
+        x[4 * q4 + 3] = v.w;
+      }
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        const float4* b = reinterpret_cast<const float4*>(stage + (c0 + q) * kGuardStageLd);
+        float s = d[q];
+#pragma unroll
+        for (int j4 = 0; j4 < 8; ++j4) {
+          const float4 v = b[j4];
+          s = fmaf(x[4 * j4 + 0], v.x, s);
+          s = fmaf(x[4 * j4 + 1], v.y, s);
+          s = fmaf(x[4 * j4 + 2], v.z, s);
+          s = fmaf(x[4 * j4 + 3], v.w, s);
+        }
+        d[q] = s;
+      }
+    }
+  }
+  bar();  // the stage may be reused once every thread is done with it
+}
+
+// One thread's share of a guarded row tile of the fused kernels: P = A - D
+// for row r0 + rl (valid below vr) and columns k0 + c0 .. + 31, D in FP32
+// from L.  P goes to pt (P^T, row stride pt_ld; skipped when pt is null)
+// and, for the diagonal rows (rl < 64) of the first tile, to the diagonal
+// block s (row stride s_ld; skipped when s is null).  Collective over NT
+// threads; kept out of line so that the unguarded path's registers do not
+// pay for it.
+template <int NT, class Bar>
+__device__ __noinline__ void guard_tile_p(const float* __restrict__ L, const float* __restrict__ A, int64_t n,
+                                          int k0, int r0, int vr, int rl, int c0, float* pt, int pt_ld, float* s,
+                                          int s_ld, float* stage, int tid, Bar bar) {
+  float d[32];
+  guard_update_row<NT>(d, L, n, k0, rl < vr ? (int64_t)(r0 + rl) : -1, c0, stage, tid, bar);
+  float p[32];
+  if (rl < vr) {
+    const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + c0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 v = src[q];
+      p[4 * q + 0] = v.x - d[4 * q + 0];
+      p[4 * q + 1] = v.y - d[4 * q + 1];
+      p[4 * q + 2] = v.z - d[4 * q + 2];
+      p[4 * q + 3] = v.w - d[4 * q + 3];
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) p[q] = 0.0f;
+  }
+  if (pt != nullptr) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) pt[(c0 + q) * pt_ld + rl] = p[q];
+  }
+  if (s != nullptr && rl < 64) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) s[rl * s_ld + c0 + q] = p[q];
+  }
+}
+
+}  // namespace b2p

@@ -22,12 +22,19 @@
 // re-read and re-written through HBM, and the update accumulates in TMEM.
 // All mbarrier waits are bounded; a timeout marks the matrix with info = -1.
 //
+// With the pivot guard (guard.cuh) the diagonal block's pivots are checked
+// after it is factored; on a failure the column's D is recomputed in FP32
+// from L (guard_tile_p) in place of the TMEM accumulator, the column is
+// redone from its first row tile, and every later column of the matrix skips
+// phase 1 and takes D from the FP32 recompute.
+//
 // The reference's left-looking paths run the same schedule through cuBLAS
 // and cuSOLVER (submission.py:3319-3409 _left_looking_large, 3606-3676,
 // 5152-5196 e62 with a resident diagonal block and inverse panel multiply).
 #include <algorithm>
 
 #include "diag64.cuh"
+#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -59,7 +66,8 @@ constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TME
 template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info) {
+                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info, int guard,
+                       int32_t* __restrict__ fp32_from) {
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
@@ -70,6 +78,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kFUnion + 48);
   int* flag = reinterpret_cast<int*>(sm + kFUnion + 56);
   int* badp = flag + 1;
+  int* gfail = flag + 2;  // the guard's verdict on the current diagonal block
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kFB;
@@ -105,12 +114,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *badp = -1;
+    int sticky = -1;  // first block column the guard recomputed in FP32
 
     for (int k = 0; k < N; ++k) {
       const int k0 = k * kFB;
       const int mtiles = (n - k0 + kFM - 1) / kFM;
       // ---------------- phase 1: left-looking update into TMEM -------------
-      if (k > 0) {
+      if (k > 0 && sticky < 0) {
         if (tid == 0) {
           const int iters = mtiles * k;
           auto load = [&](int i, int s) {
@@ -191,7 +201,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
       for (int mt = 0; mt < mtiles; ++mt) {
         const int r0 = k0 + mt * kFM;
         const int vr = min(kFM, n - r0);
-        {
+        if (k > 0 && sticky >= 0) {
+          // Guarded column: P with D in FP32 from L.  The stage is the
+          // engine's L^T scratch, idle outside the diagonal factorization.
+          const int w4 = warp & 3, h = warp >> 2;
+          guard_tile_p<kFThreads>(L, A, n, k0, r0, vr, 32 * w4 + lane, 32 * h, PtT, kFPtLd, mt == 0 ? dg.S : nullptr,
+                                  kD64Ld, diag64_lt(dg), tid, CtaBarrier());
+        } else {
           const int w4 = warp & 3, h = warp >> 2;
           const int rl = 32 * w4 + lane;
           float d[32];
@@ -231,6 +247,22 @@ __global__ void __launch_bounds__(kFThreads, 2)
           if (bad == kDiagTimeout) {
             ok = false;
             break;
+          }
+          if (guard && k > 0 && sticky < 0) {
+            if (warp == 0) {
+              const bool f =
+                  guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane);
+              if (lane == 0) *gfail = f ? 1 : 0;
+            }
+            __syncthreads();
+            const bool redo = *gfail != 0;
+            __syncthreads();
+            if (redo) {
+              // Redo the column from its first row tile with D in FP32.
+              sticky = k;
+              mt = -1;
+              continue;
+            }
           }
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
@@ -277,6 +309,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
       umma::fence_after_sync();
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
+    if (tid == 0 && fp32_from != nullptr && guard) fp32_from[b] = sticky;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
@@ -301,7 +334,7 @@ bool fused_supported(int64_t n, int mode) {
 }
 
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s) {
+                int32_t* info, cudaStream_t s, int32_t* fp32_from) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -311,13 +344,15 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const size_t smem = two ? kFSmemBytes : std::max<size_t>(kFSmemBytes, kFSmemOneCta);
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
+  const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
   TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
   if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
-    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
+    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, fp32_from);
   } else {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
-    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
+    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard,
+                                                                      fp32_from);
   }
   return check_launch("potrf_fused_kernel");
 }

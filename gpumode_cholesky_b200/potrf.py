@@ -39,23 +39,29 @@ def workspace(device: torch.device, nbytes: int) -> torch.Tensor:
 def resolve_mode(mode: str | int | None, n: int) -> int:
     """Precision mode code for order n; None picks the library default (FP32).
 
-    "auto" is BF16x3 trailing updates for n > 128 (the mixed form that meets
-    the 1e-5 relative residual) and FP32 below, where no update is blocked.
+    A name is a mode ("fp32", "tf32", "bf16x3", "fp8") optionally followed by
+    flags ("+fp64diag", "+guard").  "auto" is BF16x3 trailing updates with
+    the pivot guard for n > 128 when n is a multiple of 64 (the mixed form
+    that meets the 1e-5 relative residual; the guard recomputes in FP32 the
+    columns whose pivots the mixed update cannot resolve), and FP32
+    otherwise (orders <= 128 have no blocked update; other orders take the
+    blocked path, which has no guard).
     """
     if mode is None:
         return _lib.MODE_FP32
     if isinstance(mode, int):
         return mode
-    flags = 0
-    name = mode.lower()
-    if name == "auto":
-        return _lib.MODE_BF16X3 if n > 128 else _lib.MODE_FP32
-    if name.endswith("+fp64diag"):
-        flags = _lib.FLAG_FP64_DIAG
-        name = name[: -len("+fp64diag")]
+    name, *flags = mode.lower().split("+")
+    if name == "auto" and not flags:
+        return (_lib.MODE_BF16X3 | _lib.FLAG_GUARD) if n > 128 and n % 64 == 0 else _lib.MODE_FP32
     if name not in _lib.MODES:
         raise ValueError(f"unknown precision mode {mode!r}; expected one of {sorted(_lib.MODES)}")
-    return _lib.MODES[name] | flags
+    code = _lib.MODES[name]
+    for f in flags:
+        if f not in _lib.FLAGS:
+            raise ValueError(f"unknown mode flag {f!r} in {mode!r}; expected one of {sorted(_lib.FLAGS)}")
+        code |= _lib.FLAGS[f]
+    return code
 
 
 def _check_input(a: torch.Tensor) -> None:
@@ -75,14 +81,19 @@ def cholesky(
     out: torch.Tensor | None = None,
     info: torch.Tensor | None = None,
     path: str = "auto",
+    fp32_from: torch.Tensor | None = None,
 ) -> torch.Tensor:
     """Factor a batch of SPD matrices: returns L with A = L L^T.
 
     ``mode`` selects the trailing-update arithmetic ("fp32", "tf32",
-    "bf16x3", "fp8", optionally suffixed "+fp64diag").  ``info`` may be an
-    int32 CUDA tensor of shape (batch,) that receives 0 or the 1-based index
-    of the first non-positive pivot.  ``path`` forces the algorithm for
-    n > 128 ("blocked", "fused", "fused_ws", "split"; default "auto").
+    "bf16x3", "fp8", optionally suffixed "+fp64diag" and/or "+guard"; "auto"
+    is "bf16x3+guard" for orders > 128 that are multiples of 64, else
+    "fp32").  ``info`` may be an int32 CUDA tensor of shape (batch,) that
+    receives 0 or the 1-based index of the first non-positive pivot.
+    ``fp32_from`` may be an int32 CUDA tensor of shape (batch,) that receives
+    the first 64-wide block column the pivot guard recomputed in FP32, or -1.
+    ``path`` forces the algorithm for n > 128 ("blocked", "fused",
+    "fused_ws", "split"; default "auto").
     """
     if path not in _lib.PATHS:
         raise ValueError(f"unknown path {path!r}; expected one of {sorted(_lib.PATHS)}")
@@ -104,10 +115,16 @@ def cholesky(
             if info.dtype != torch.int32 or info.numel() < batch or not info.is_cuda:
                 raise ValueError("info must be an int32 CUDA tensor with at least batch elements")
             info_ptr = info.data_ptr()
-        st = lib.b2p_potrf_batched_path(
-            a.data_ptr(), out.data_ptr(), batch, n, code, pcode, ws_ptr, ws_bytes, info_ptr, _stream_ptr(a.device)
+        from_ptr = None
+        if fp32_from is not None:
+            if fp32_from.dtype != torch.int32 or fp32_from.numel() < batch or not fp32_from.is_cuda:
+                raise ValueError("fp32_from must be an int32 CUDA tensor with at least batch elements")
+            from_ptr = fp32_from.data_ptr()
+        st = lib.b2p_potrf_batched_ex(
+            a.data_ptr(), out.data_ptr(), batch, n, code, pcode, ws_ptr, ws_bytes, info_ptr, from_ptr,
+            _stream_ptr(a.device),
         )
-    _lib.check(st, "b2p_potrf_batched_path")
+    _lib.check(st, "b2p_potrf_batched_ex")
     return out
 
 
@@ -237,6 +254,10 @@ def cholesky_checked(
 def custom_kernel(data: torch.Tensor) -> torch.Tensor:
     """Drop-in for the reference entry point ``custom_kernel`` (submission.py:4101).
 
-    One library call on the current stream, no host synchronisation.
+    One library call on the current stream, no host synchronisation, in the
+    "auto" mode: BF16x3 trailing updates with the pivot guard for orders
+    > 128 that are multiples of 64 (the reference likewise routes its
+    benchmark shapes to mixed TF32/FP16/FP8 products), plain FP32 otherwise.
+    ``cholesky(data, mode="fp32")`` is the plain FP32 method.
     """
-    return cholesky(data)
+    return cholesky(data, mode="auto")

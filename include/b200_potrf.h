@@ -60,6 +60,22 @@ extern "C" {
  * diagonal tiles); orders <= 128 ignore the flag.  No counterpart exists in
  * the reference.                                                             */
 #define B2P_FLAG_FP64_DIAG 0x100
+/* Flag OR-ed into a tensor mode: the pivot guard.  After the 64 x 64
+ * diagonal block of each block column is factored, every pivot is checked
+ * against the error the mixed update can carry:
+ *     L_jj^2 > 2 (delta + s 2^-23) A_jj,
+ * delta = 2^-16 for BF16x3 and 2^-10 for TF32 (operand rounding), s the
+ * tensor-core accumulation steps so far (one FP32 ulp each).  A column with
+ * a failing (or non-positive, or non-finite) pivot is recomputed with its
+ * update in FP32 on the SIMT cores, from the FP32 factor already written, and
+ * so is every later column of that matrix, so that from there on the matrix
+ * is factored as by B2P_MODE_FP32.  No host synchronisation is involved.
+ * The fused, warp-specialized and split paths (n % 64 == 0) honour it; the
+ * blocked path ignores it.  The reference's analogue is the accurate retry
+ * of its 256-order kernel when a pivot falls under 1e-2 of the input's
+ * diagonal (submission.py:866-886, 1004-1031), which refactors the whole
+ * matrix.                                                                    */
+#define B2P_FLAG_GUARD 0x200
 
 /* Library version as major*10000 + minor*100 + patch. */
 B2P_API int b2p_version(void);
@@ -116,6 +132,18 @@ B2P_API int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n
 B2P_API size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int path);
 B2P_API int b2p_potrf_batched_path(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
                                    void* workspace, size_t workspace_bytes, int32_t* info, void* stream);
+
+/*
+ * b2p_potrf_batched_path with one more optional output: fp32_from, a device
+ * int32[batch] receiving per matrix the first block column (0-based, 64
+ * columns each) from which B2P_FLAG_GUARD recomputed the update in FP32, or
+ * -1 when it recomputed none (always -1 without the flag, on the blocked
+ * path and for n <= 128).  The same call as b2p_potrf_batched_path
+ * otherwise; the workspace query is b2p_potrf_path_workspace_size.
+ */
+B2P_API int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int mode, int path,
+                                 void* workspace, size_t workspace_bytes, int32_t* info, int32_t* fp32_from,
+                                 void* stream);
 
 /*
  * Host-resident batches: factors a (batch, n, n) FP32 batch held in HOST

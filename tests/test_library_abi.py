@@ -174,11 +174,18 @@ def test_error_raises_python_exception():
 def test_mode_names():
     assert resolve_mode(None, 512) == _lib.MODE_FP32
     assert resolve_mode("bf16x3", 512) == _lib.MODE_BF16X3
-    assert resolve_mode("auto", 512) == _lib.MODE_BF16X3
+    # auto: BF16x3 with the pivot guard where the guarded paths run (orders
+    # > 128, multiples of 64), FP32 elsewhere.
+    assert resolve_mode("auto", 512) == _lib.MODE_BF16X3 | _lib.FLAG_GUARD
+    assert resolve_mode("auto", 300) == _lib.MODE_FP32
     assert resolve_mode("auto", 128) == _lib.MODE_FP32
     assert resolve_mode("tf32+fp64diag", 512) == _lib.MODE_TF32 | _lib.FLAG_FP64_DIAG
+    assert resolve_mode("bf16x3+guard", 512) == _lib.MODE_BF16X3 | _lib.FLAG_GUARD
+    assert resolve_mode("tf32+guard+fp64diag", 512) == _lib.MODE_TF32 | _lib.FLAG_GUARD | _lib.FLAG_FP64_DIAG
     with pytest.raises(ValueError):
         resolve_mode("int8", 512)
+    with pytest.raises(ValueError):
+        resolve_mode("bf16x3+fast", 512)
 
 
 def test_custom_kernel_rejects_cpu_input():

@@ -93,7 +93,10 @@ def test_nonspd_info_all_paths(n):
 
 @pytest.mark.parametrize("batch,n", [(4096, 32), (1024, 64), (256, 128), (640, 512), (60, 1024), (8, 2048)])
 def test_full_size_properties(batch, n):
-    """Benchmark shapes: relative residual in FP64 on the device, triangularity, positive diagonal."""
+    """Benchmark shapes through the drop-in: relative residual in FP64 on the
+    device, triangularity, positive diagonal.  Orders <= 128 run plain FP32
+    (residual < 2e-6); the others run BF16x3 with the pivot guard, held to the
+    mixed modes' 1e-5."""
     a = inputs.well_conditioned(batch, n, seed=n, device="cuda")
     l = custom_kernel(a)
     assert torch.isfinite(l).all()
@@ -101,7 +104,7 @@ def test_full_size_properties(batch, n):
     assert (torch.diagonal(l, dim1=-2, dim2=-1) > 0).all()
     ld = l.double()
     r = torch.linalg.matrix_norm(ld @ ld.transpose(-1, -2) - a.double()) / torch.linalg.matrix_norm(a.double())
-    assert r.max().item() < 2e-6
+    assert r.max().item() < (2e-6 if n <= 128 else 1e-5)
 
 
 @pytest.mark.parametrize("mode", ["fp32+fp64diag", "bf16x3+fp64diag"])
@@ -125,3 +128,50 @@ def test_fp64_diagonal_tiles(mode, batch, n):
     cholesky(bad.cuda(), mode=mode, info=info)
     want = oracle.potrf_f64(bad.numpy())[1]
     assert np.array_equal(info.cpu().numpy(), want)
+
+
+# Mixed modes against the same FP64 oracle.  The golden cases that reach the
+# tensor-core kernels (orders > 128 that are multiples of 64), then the
+# reference's input families at orders 512 and 1024, where the reference's
+# own error is that of its FP32 route restated by the oracle (LAPACK's
+# column Cholesky in FP32, oracle.potrf_f32).  Same bound as the FP32 parity:
+# ||L - L64|| <= 4 x the reference's error + 1e-6.
+MIXED_GOLDEN = [c for c in GOLDEN_CASES if c["n"] > 128 and c["n"] % 64 == 0]
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "auto"])
+@pytest.mark.parametrize("c", MIXED_GOLDEN, ids=case_id)
+def test_golden_parity_mixed(c, mode):
+    a = torch.from_numpy(c["a"]).cuda()
+    info = torch.full((c["batch"],), -7, dtype=torch.int32, device="cuda")
+    l = cholesky(a, mode=mode, info=info)
+    torch.cuda.synchronize()
+    ln = l.cpu().numpy()
+    ok, msg = oracle.check_implementation(c["a"], ln)
+    assert ok, msg
+    assert np.all(np.triu(ln, 1) == 0.0)
+    assert np.array_equal(info.cpu().numpy(), c["info"])
+    l64, _ = oracle.potrf_f64(c["a"])
+    ours = _rel_err(ln, l64).max()
+    ref = _rel_err(c["l"], l64).max()
+    assert ours <= 4.0 * ref + 1e-6, (ours, ref)
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "auto"])
+@pytest.mark.parametrize(
+    "batch,n,cond,case",
+    [(4, 512, 2, "dense"), (4, 512, 5, "spectrum"), (4, 512, 4, "lowrank"), (4, 512, 4, "rowscale"),
+     (2, 1024, 2, "dense"), (2, 1024, 5, "spectrum"), (2, 1024, 4, "lowrank")],
+)
+def test_reference_families_mixed(batch, n, cond, case, mode):
+    a = inputs.generate_input(batch, n, cond, 4000 + n + cond, case, device="cpu")
+    an = a.numpy()
+    info = torch.full((batch,), -7, dtype=torch.int32, device="cuda")
+    ln = cholesky(a.cuda(), mode=mode, info=info).cpu().numpy()
+    ok, msg = oracle.check_implementation(an, ln)
+    assert ok, msg
+    l64, want_info = oracle.potrf_f64(an)
+    assert np.array_equal(info.cpu().numpy(), want_info)
+    ref32, _ = oracle.potrf_f32(an)
+    ours, ref = _rel_err(ln, l64).max(), _rel_err(ref32, l64).max()
+    assert ours <= 4.0 * ref + 1e-6, (ours, ref)
