@@ -17,15 +17,19 @@
 // The guard therefore checks, after the diagonal block of column k is
 // factored, every pivot against
 //     d_j = L_jj^2  >  kGuardMargin * delta(k) * A_jj
-// (non-finite or non-positive pivots fail too).  When one fails, the column's
-// update is recomputed in FP32 on the SIMT cores from the FP32 factor already
-// written (L[:, 0:k0] is final), the column is refactored from it, and every
-// later column of that matrix is computed the same way: after the first
-// failure the factorization continues as the plain FP32 method would.  The
-// reference's closest analogue is the accurate retry of its 256-order kernel,
-// triggered when a pivot falls under 1e-2 of the input's diagonal
-// (submission.py:866-868, 883-886, 1004-1031), which refactors the whole
-// matrix in FP32.
+// (non-finite or non-positive pivots fail too) and records the first
+// failing column of each matrix.  A matrix that trips is then refactored
+// from its first column in FP32 on the SIMT cores (potrf_rescue.cu), in one
+// more launch that does nothing when no matrix tripped.  Recomputing only
+// from the failing column on is not enough: the mixed columns before it
+// already carry a backward error of about delta * |A|, which can exceed the
+// smallest eigenvalues of the remaining Schur complement (on the Gaussian-
+// process kernels of order 2048 an FP32 recompute from the failing column on
+// still met a negative pivot, while a restart from column 0 gave the FP32
+// residual).  The reference's closest analogue is the accurate retry of its
+// 256-order kernel, triggered when a pivot falls under 1e-2 of the input's
+// diagonal (submission.py:866-868, 883-886, 1004-1031), which likewise
+// refactors the whole matrix in FP32.
 #pragma once
 
 #include <stdint.h>
@@ -69,7 +73,8 @@ __device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, con
 
 // FP32 update of one row against 32 columns of block column k, computed on
 // the SIMT cores: d[q] = sum_{j < k0} L[row][j] * L[k0 + c0 + q][j] (in order
-// of increasing j, fused multiply-adds).  Collective over the NT threads
+// of increasing j, fused multiply-adds).  L is read through L2 only: other
+// CTAs of the same launch write it.  Collective over the NT threads
 // that call it (barrier functor `bar`): each passes its own row (-1 for
 // none; d is then 0) and c0 (0 or 32, uniform within a warp); `stage` holds
 // kGuardStageFloats floats of shared memory, free until the call returns.
@@ -83,7 +88,7 @@ __device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __
     for (int e = tid; e < 64 * 8; e += NT) {
       const int c = e >> 3, q4 = e & 7;
       *reinterpret_cast<float4*>(stage + c * kGuardStageLd + 4 * q4) =
-          *reinterpret_cast<const float4*>(L + (size_t)(k0 + c) * n + j0 + 4 * q4);
+          __ldcg(reinterpret_cast<const float4*>(L + (size_t)(k0 + c) * n + j0 + 4 * q4));
     }
     bar();
     if (row >= 0) {
@@ -91,7 +96,7 @@ __device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __
       const float4* src = reinterpret_cast<const float4*>(L + (size_t)row * n + j0);
 #pragma unroll
       for (int q4 = 0; q4 < 8; ++q4) {
-        const float4 v = src[q4];
+        const float4 v = __ldcg(src + q4);
         x[4 * q4 + 0] = v.x;
         x[4 * q4 + 1] = v.y;
         x[4 * q4 + 2] = v.z;
@@ -116,41 +121,24 @@ __device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __
   bar();  // the stage may be reused once every thread is done with it
 }
 
-// One thread's share of a guarded row tile of the fused kernels: P = A - D
-// for row r0 + rl (valid below vr) and columns k0 + c0 .. + 31, D in FP32
-// from L.  P goes to pt (P^T, row stride pt_ld; skipped when pt is null)
-// and, for the diagonal rows (rl < 64) of the first tile, to the diagonal
-// block s (row stride s_ld; skipped when s is null).  Collective over NT
-// threads; kept out of line so that the unguarded path's registers do not
-// pay for it.
+// One thread's share of the FP32 recompute of P = A - D for its row `row`
+// (-1: none) and columns k0 + c0 .. + 31 of block column k: D in FP32 from
+// L (guard_update_row), P into dst[0..31] (shared memory).  Collective over
+// NT threads.
 template <int NT, class Bar>
-__device__ __noinline__ void guard_tile_p(const float* __restrict__ L, const float* __restrict__ A, int64_t n,
-                                          int k0, int r0, int vr, int rl, int c0, float* pt, int pt_ld, float* s,
-                                          int s_ld, float* stage, int tid, Bar bar) {
+__device__ __forceinline__ void guard_row_p(const float* __restrict__ L, const float* __restrict__ A, int64_t n,
+                                            int k0, int64_t row, int c0, float* dst, float* stage, int tid,
+                                            Bar bar) {
   float d[32];
-  guard_update_row<NT>(d, L, n, k0, rl < vr ? (int64_t)(r0 + rl) : -1, c0, stage, tid, bar);
-  float p[32];
-  if (rl < vr) {
-    const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + c0);
+  guard_update_row<NT>(d, L, n, k0, row, c0, stage, tid, bar);
+  if (row >= 0) {
+    const float4* src = reinterpret_cast<const float4*>(A + (size_t)row * n + k0 + c0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const float4 v = src[q];
-      p[4 * q + 0] = v.x - d[4 * q + 0];
-      p[4 * q + 1] = v.y - d[4 * q + 1];
-      p[4 * q + 2] = v.z - d[4 * q + 2];
-      p[4 * q + 3] = v.w - d[4 * q + 3];
+      reinterpret_cast<float4*>(dst)[q] =
+          make_float4(v.x - d[4 * q], v.y - d[4 * q + 1], v.z - d[4 * q + 2], v.w - d[4 * q + 3]);
     }
-  } else {
-#pragma unroll
-    for (int q = 0; q < 32; ++q) p[q] = 0.0f;
-  }
-  if (pt != nullptr) {
-#pragma unroll
-    for (int q = 0; q < 32; ++q) pt[(c0 + q) * pt_ld + rl] = p[q];
-  }
-  if (s != nullptr && rl < 64) {
-#pragma unroll
-    for (int q = 0; q < 32; ++q) s[rl * s_ld + c0 + q] = p[q];
   }
 }
 

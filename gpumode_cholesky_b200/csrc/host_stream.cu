@@ -110,7 +110,7 @@ int b2p_potrf_batched_host(const float* host_a, float* host_l, int64_t batch, in
   if (batch < 0 || n < 0 || n > (1 << 20) || chunk < 0)
     return set_error(B2P_ERR_INVALID_ARG, "bad shape batch=%lld n=%lld chunk=%lld", (long long)batch, (long long)n,
                      (long long)chunk);
-  if ((mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG)) != 0 || (mode & B2P_MODE_MASK) > B2P_MODE_FP8)
+  if ((mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG | B2P_FLAG_GUARD)) != 0 || (mode & B2P_MODE_MASK) > B2P_MODE_FP8)
     return set_error(B2P_ERR_INVALID_ARG, "unknown mode 0x%x", mode);
   if (batch == 0 || n == 0) return B2P_OK;
   if (host_a == nullptr || host_l == nullptr) return set_error(B2P_ERR_INVALID_ARG, "null matrix pointer");

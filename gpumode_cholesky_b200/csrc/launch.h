@@ -54,6 +54,15 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
 bool fused_ws_fits(int64_t batch, int64_t n, int mode);
 bool fused_ws_supported(int64_t batch, int64_t n, int mode);
 
+// Pivot guard (guard.cuh, potrf_rescue.cu).  A guarded call keeps, after
+// its path's own workspace, guard_ws_bytes(batch): the per-matrix guard
+// state (int32: first failing block column, -1 for none; the caller's
+// fp32_from array takes its place when given) and two barrier words.
+// guard_rescue refactors in FP32 every matrix whose state is >= 0.
+size_t guard_ws_bytes(int64_t batch);
+int guard_rescue(const float* a, float* l, int64_t batch, int n, const int32_t* gstate, int* bar, int32_t* info,
+                 cudaStream_t s);
+
 // Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
 // n > 128, tensor modes; two launches per 64-wide block column.
 bool split_supported(int64_t n, int mode);
@@ -132,6 +141,7 @@ enum KernelId {
   kKTrsv,
   kKGpForward,
   kKGpLbar,
+  kKRescue,
   kKCount
 };
 
@@ -190,6 +200,7 @@ enum SmemSlot {
   kSlotTrsv0,
   kSlotTrsv1,
   kSlotGpForward,
+  kSlotRescue,
   kSlotCount
 };
 

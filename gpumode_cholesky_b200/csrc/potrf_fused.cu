@@ -22,11 +22,10 @@
 // re-read and re-written through HBM, and the update accumulates in TMEM.
 // All mbarrier waits are bounded; a timeout marks the matrix with info = -1.
 //
-// With the pivot guard (guard.cuh) the diagonal block's pivots are checked
-// after it is factored; on a failure the column's D is recomputed in FP32
-// from L (guard_tile_p) in place of the TMEM accumulator, the column is
-// redone from its first row tile, and every later column of the matrix skips
-// phase 1 and takes D from the FP32 recompute.
+// With the pivot guard (guard.cuh) warp 0 checks the diagonal block's pivots
+// once it is factored and records the first failing column of the matrix;
+// the call then runs the FP32 rescue (potrf_rescue.cu) for the matrices
+// that tripped.
 //
 // The reference's left-looking paths run the same schedule through cuBLAS
 // and cuSOLVER (submission.py:3319-3409 _left_looking_large, 3606-3676,
@@ -67,7 +66,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
                        uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info, int guard,
-                       int32_t* __restrict__ fp32_from) {
+                       int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
@@ -78,7 +77,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kFUnion + 48);
   int* flag = reinterpret_cast<int*>(sm + kFUnion + 56);
   int* badp = flag + 1;
-  int* gfail = flag + 2;  // the guard's verdict on the current diagonal block
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kFB;
@@ -114,13 +112,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *badp = -1;
-    int sticky = -1;  // first block column the guard recomputed in FP32
+    bool tripped = false;  // warp 0: the guard has recorded a column of this matrix
 
     for (int k = 0; k < N; ++k) {
       const int k0 = k * kFB;
       const int mtiles = (n - k0 + kFM - 1) / kFM;
       // ---------------- phase 1: left-looking update into TMEM -------------
-      if (k > 0 && sticky < 0) {
+      if (k > 0) {
         if (tid == 0) {
           const int iters = mtiles * k;
           auto load = [&](int i, int s) {
@@ -201,13 +199,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
       for (int mt = 0; mt < mtiles; ++mt) {
         const int r0 = k0 + mt * kFM;
         const int vr = min(kFM, n - r0);
-        if (k > 0 && sticky >= 0) {
-          // Guarded column: P with D in FP32 from L.  The stage is the
-          // engine's L^T scratch, idle outside the diagonal factorization.
-          const int w4 = warp & 3, h = warp >> 2;
-          guard_tile_p<kFThreads>(L, A, n, k0, r0, vr, 32 * w4 + lane, 32 * h, PtT, kFPtLd, mt == 0 ? dg.S : nullptr,
-                                  kD64Ld, diag64_lt(dg), tid, CtaBarrier());
-        } else {
+        {
           const int w4 = warp & 3, h = warp >> 2;
           const int rl = 32 * w4 + lane;
           float d[32];
@@ -248,21 +240,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
             ok = false;
             break;
           }
-          if (guard && k > 0 && sticky < 0) {
-            if (warp == 0) {
-              const bool f =
-                  guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane);
-              if (lane == 0) *gfail = f ? 1 : 0;
-            }
-            __syncthreads();
-            const bool redo = *gfail != 0;
-            __syncthreads();
-            if (redo) {
-              // Redo the column from its first row tile with D in FP32.
-              sticky = k;
-              mt = -1;
-              continue;
-            }
+          if (guard && k > 0 && warp == 0 && !tripped &&
+              guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane)) {
+            tripped = true;
+            if (lane == 0) gstate[b] = k;
           }
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
@@ -309,7 +290,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
       umma::fence_after_sync();
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
-    if (tid == 0 && fp32_from != nullptr && guard) fp32_from[b] = sticky;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
@@ -322,9 +302,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
   if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
 }
 
-// The workspace pointer is rounded up to 1024 bytes inside, hence the slack.
+// The panel copies, then the pivot guard's area; the workspace pointer is
+// rounded up to 1024 bytes inside, hence the slack.
 size_t fused_workspace_bytes(int64_t batch, int64_t n) {
-  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 1024;
+  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + guard_ws_bytes(batch) + 1024;
 }
 
 bool fused_supported(int64_t n, int mode) {
@@ -345,16 +326,27 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
   const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
-  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
-    if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
-    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, fp32_from);
-  } else {
-    if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
-    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard,
-                                                                      fp32_from);
+  uint8_t* garea = wsa + (size_t)batch * 2 * panel_copy_region_bytes(n);
+  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
+  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
+  if (guard) {
+    const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
   }
-  return check_launch("potrf_fused_kernel");
+  {
+    TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
+    if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
+      if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
+      potrf_fused_kernel<B2P_MODE_TF32>
+          <<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, gstate);
+    } else {
+      if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
+      potrf_fused_kernel<B2P_MODE_BF16X3>
+          <<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, gstate);
+    }
+  }
+  if (int st = check_launch("potrf_fused_kernel")) return st;
+  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
 }
 
 }  // namespace b2p

@@ -31,12 +31,9 @@
 // marks the matrix with info = -1 and drains outstanding copies and MMAs
 // before TMEM is released.
 //
-// Pivot guard (guard.cuh): every CTA checks the pivots of its (identical)
-// copy of the diagonal block; on a failure the consumers redo tile 0 with D
-// recomputed in FP32 from L, and take D that way for every later tile of
-// the matrix.  The producer is not told: its accumulators are still waited
-// for and released, so the barrier phases stay as they are, and only their
-// values go unused.
+// With the pivot guard (guard.cuh) warp 0 of rank 0 checks the diagonal
+// block's pivots and records the first failing column of the matrix; the
+// call then runs the FP32 rescue (potrf_rescue.cu) for those matrices.
 //
 // The reference's left-looking paths (submission.py:3319-3409, 3606-3676,
 // 5152-5196) issue the same three phases as separate cuSOLVER / cuBLAS /
@@ -242,7 +239,7 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
 // Consumers: warps 0-7.
 template <int MODE, int CL>
 __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
-                             int n, uint32_t tmem, int32_t* info, int rank, int guard, int32_t* fp32_from) {
+                             int n, uint32_t tmem, int32_t* info, int rank, int guard, int32_t* gstate) {
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
@@ -259,7 +256,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *br.badp = -1;
     bool failed = false;
-    int sticky = -1;  // first block column the guard recomputed in FP32
+    bool tripped = false;  // warp 0: the guard has recorded a column of this matrix
     for (int k = 0; k < N && !failed; ++k) {
       const int k0 = k * kWB;
       const int mt_n = (n - k0 + kWM - 1) / kWM;
@@ -270,33 +267,21 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
         const bool diag_only = CL > 1 && rank != 0 && mt == 0;
         const int r0 = k0 + mt * kWM;
         const int vr = diag_only ? 64 : min(kWM, n - r0);
-        // Two passes only when the guard rejects the diagonal block.
-        for (int pass = 0;; ++pass) {
-        // (a) D from TMEM (or, guarded, in FP32 from L), P = A - D.
+        // (a) D from TMEM, P = A - D.
         {
           const int w4 = warp & 3, h = warp >> 2;
           const int rl = 32 * w4 + lane;
-          if (k > 0 && pass == 0) {
+          float d[32];
+          if (k > 0) {
             const bool got = ws_wait(br.acc_ready + j, (ready_par >> j) & 1u, br.flag);
             ready_par ^= 1u << j;
             if (!got) *br.flag = 1;
           }
-          if (pass == 0) cbar();
+          cbar();
           if (*br.flag) {
             failed = true;
             break;
           }
-          if (k > 0 && sticky >= 0) {
-            // Guarded: the accumulator is released unread and P is formed
-            // with D in FP32 from L (the stage is the engine's idle L^T scratch).
-            if (pass == 0) {
-              __syncwarp();
-              if (lane == 0) mbar_arrive(br.acc_free + j);
-            }
-            guard_tile_p<kWConsumers>(L, A, n, k0, r0, vr, rl, 32 * h, diag_only ? nullptr : PtT, kWPtLd,
-                                      mt == 0 ? dg.S : nullptr, kD64Ld, diag64_lt(dg), tid, cbar);
-          } else {
-          float d[32];
           if (k > 0) {
             umma::fence_after_sync();
             umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kWB * j + 32 * h), d);
@@ -330,7 +315,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
           }
-          }
         }
         cbar();
         // (b) diagonal block: L_kk and T^T (pipelined engine), zero strip.
@@ -340,20 +324,10 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             failed = true;
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
-          if (guard && k > 0 && sticky < 0 && bad != kDiagTimeout) {
-            int* gfail = const_cast<int*>(br.flag) + 2;
-            if (warp == 0) {
-              const bool f =
-                  guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane);
-              if (lane == 0) *gfail = f ? 1 : 0;
-            }
-            cbar();
-            const bool redo = *gfail != 0;
-            cbar();
-            if (redo) {
-              sticky = k;
-              continue;  // second pass over tile 0 with D in FP32
-            }
+          if (guard && k > 0 && rank == 0 && warp == 0 && !tripped && bad != kDiagTimeout &&
+              guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane)) {
+            tripped = true;
+            if (lane == 0) gstate[b] = k;
           }
           if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
           for (int e = tid; e < (rank == 0 ? 64 * 16 : 0); e += kWConsumers) {
@@ -376,9 +350,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           }
           cbar();
         }
-        break;
-        }
-        if (failed) break;
         if (diag_only) continue;
         // (c) X = P T^T (triangle skipped), then L and the tensor-core copy from X^T.
         xgemm_tri_inplace(PtT, kWPtLd, dg.T, kD64Ld, cbar);
@@ -414,7 +385,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
       }
     }
     if (tid == 0 && rank == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
-    if (tid == 0 && rank == 0 && fp32_from != nullptr && guard) fp32_from[b] = sticky;
     if (failed) break;
   }
   // The strip's bulk stores read the zero buffer until they complete.
@@ -425,7 +395,7 @@ template <int MODE, int CL>
 __global__ void __launch_bounds__(kWThreads, 1)
     potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
                           uint8_t* __restrict__ ws, int32_t* __restrict__ info, int guard,
-                          int32_t* __restrict__ fp32_from) {
+                          int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char wraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wraw) + 1023) & ~(uintptr_t)1023);
   WsBars br;
@@ -467,7 +437,7 @@ __global__ void __launch_bounds__(kWThreads, 1)
   if (warp == kWConsumers / 32) {
     if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
-    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank, guard, fp32_from);
+    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank, guard, gstate);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -536,11 +506,20 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
   const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, guard, fp32_from);
-  if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
-  return B2P_OK;
+  uint8_t* garea = wsa + (size_t)batch * 2 * panel_copy_region_bytes(n);
+  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
+  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
+  if (guard) {
+    const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
+  }
+  {
+    TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, guard, gstate);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
+  }
+  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
 }
 
 }  // namespace b2p

@@ -223,8 +223,12 @@ int b2p_ragged_plan_create_ex(const int64_t* offsets_host, const int32_t* n_host
   if (count < 0 || (count > 0 && (offsets_host == nullptr || n_host == nullptr)))
     return set_error(B2P_ERR_INVALID_ARG, "bad ragged list");
   const int m = mode & B2P_MODE_MASK;
-  if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG)))
+  if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG | B2P_FLAG_GUARD)))
     return set_error(B2P_ERR_INVALID_ARG, "unknown mode 0x%x", mode);
+  // The pivot guard is not applied to ragged batches: its FP32 rescue is a
+  // cooperative launch over every SM, and the ragged groups run on several
+  // streams at once.  The flag is accepted and ignored.
+  mode &= ~B2P_FLAG_GUARD;
   if (m == B2P_MODE_FP8 || (mode & B2P_FLAG_FP64_DIAG))
     return set_error(B2P_ERR_UNSUPPORTED, "ragged batches support fp32, tf32 and bf16x3");
   const bool tensor = (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3);

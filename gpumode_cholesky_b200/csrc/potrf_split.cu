@@ -486,63 +486,15 @@ constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the
 // the CTA's 128-row chunks by forward substitution (one row per thread,
 // which is also one TMEM lane per thread), write L and the panel copy.
 //
-// Guarded chunk rows (out of line, so that the unguarded path's registers do
-// not pay for it): P = A - D for row r (< n) with D in FP32 from L, 32
-// columns at a time into the row's own shared-memory slice of the stage
-// (kSThreads x 68 floats after the 64-row update stage), then the same solve,
-// L and panel-copy stores as the tensor-core form.  Collective over the CTA.
-template <int MODE>
-__device__ __noinline__ void split_guard_rows(float* __restrict__ L, const float* __restrict__ Ab, int n, int k0,
-                                              int r, const Diag64Smem& dg, float* stage, uint8_t* W0, uint8_t* W1,
-                                              int tid) {
-  const int N = n / 64, k = k0 / 64;
-  float* xs = stage + kGuardStageFloats + tid * 68;  // this thread's P row
-  for (int h = 0; h < 2; ++h) {
-    float d[32];
-    guard_update_row<kSThreads>(d, L, n, k0, r < n ? (int64_t)r : -1, 32 * h, stage, tid, CtaBarrier());
-    if (r < n) {
-      const float4* src = reinterpret_cast<const float4*>(Ab + (size_t)r * n + k0 + 32 * h);
-#pragma unroll
-      for (int c4 = 0; c4 < 8; ++c4) {
-        const float4 v = src[c4];
-        reinterpret_cast<float4*>(xs + 32 * h)[c4] =
-            make_float4(v.x - d[4 * c4], v.y - d[4 * c4 + 1], v.z - d[4 * c4 + 2], v.w - d[4 * c4 + 3]);
-      }
-    }
-  }
-  if (r < n) {
-    float x[64];
-#pragma unroll
-    for (int c = 0; c < 64; ++c) x[c] = xs[c];
-    panel_solve64(x, dg);
-    float4* dst = reinterpret_cast<float4*>(L + (size_t)r * n + k0);
-#pragma unroll
-    for (int c4 = 0; c4 < 16; ++c4) dst[c4] = make_float4(x[4 * c4], x[4 * c4 + 1], x[4 * c4 + 2], x[4 * c4 + 3]);
-    if (k + 1 < N) {
-#pragma unroll
-      for (int c8 = 0; c8 < 8; ++c8) {
-        const float v[8] = {x[8 * c8],     x[8 * c8 + 1], x[8 * c8 + 2], x[8 * c8 + 3],
-                            x[8 * c8 + 4], x[8 * c8 + 5], x[8 * c8 + 6], x[8 * c8 + 7]};
-        panel_copy_store<MODE>(W0, W1, N, k, r, c8, v);
-      }
-    }
-  }
-  __syncthreads();
-}
-
-//
-// Pivot guard (guard.cuh): gstate[b] holds the first block column of matrix
-// b recomputed in FP32 (-1: none).  Every CTA of matrix b checks its copy of
-// the diagonal block; all copies are equal, so all CTAs agree.  On a
-// failure they record k, refactor the diagonal block from P recomputed in
-// FP32 from A and L, and take the panel rows the same way; later steps read
-// gstate[b] and go straight to the FP32 form (values written during this
-// launch are k itself, so reading them races with nothing that matters).
+// With the pivot guard (guard.cuh), warp 0 of the matrix's first CTA (g = 0)
+// checks the factored diagonal block, unless an earlier step has already
+// recorded a column for the matrix, and records k on a failure; the call
+// runs the FP32 rescue (potrf_rescue.cu) after its last step.
 template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info, int guard, int32_t* gstate) {
+                      int32_t* __restrict__ info, int guard, int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -550,11 +502,6 @@ __global__ void __launch_bounds__(kSThreads, 1)
   uint64_t* done = full + 1;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSBar + 16);
   int* flag = reinterpret_cast<int*>(sm + kSBar + 24);
-  int* gfail = flag + 1;
-  // The guard's stage: the operand staging (bytes 0 .. kSZero), idle whenever
-  // the guard runs (no MMA is in flight then).
-  float* gstage = reinterpret_cast<float*>(sm + kSB);
-  static_assert((kGuardStageFloats + kSThreads * 68) * 4 <= kSZero, "guard stage fits the operand staging");
   const int tid = threadIdx.x, warp = tid >> 5;
   const int N = n / 64, k0 = 64 * k;
   const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
@@ -590,13 +537,6 @@ __global__ void __launch_bounds__(kSThreads, 1)
     uint8_t* W1 = W0 + rbytes;
     const float* base = (k >= 2) ? pbuf + (size_t)b * n * 64 : a + (size_t)b * n2 + k0;
     const size_t bld = (k >= 2) ? 64 : (size_t)n;
-    const float* Ab = a + (size_t)b * n2;
-    // Guarded matrix whose FP32 recompute began at an earlier column.
-    bool fp = false;
-    if (guard && upd) {
-      const int v = *reinterpret_cast<volatile const int*>(gstate + b);
-      fp = v >= 0 && v < k;
-    }
 
     // The newest panel's product for the diagonal rows and chunk q (or the
     // diagonal rows only when q is out of range); false on a timeout.
@@ -638,17 +578,12 @@ __global__ void __launch_bounds__(kSThreads, 1)
     };
 
     // 1. Diagonal block: P_kk = base - D (rows k0..k0+63), into dg.S.
-    if (upd && !fp && !newest_panel(g, true)) {
+    if (upd && !newest_panel(g, true)) {
       ok = false;
       if (tid == 0 && info != nullptr) info[b] = -1;
       break;
     }
-    if (fp) {
-      // Guarded: P_kk = A - D with D in FP32 from L.
-      for (int h = 0; h < 2; ++h)
-        guard_tile_p<kSThreads>(L, Ab, n, k0, k0, 64, tid, 32 * h, nullptr, 0, dg.S, kD64Ld, gstage, tid,
-                                CtaBarrier());
-    } else if (warp < 2) {
+    if (warp < 2) {
       const float4* src = reinterpret_cast<const float4*>(base + (size_t)(k0 + tid) * bld);
       float4* dst = reinterpret_cast<float4*>(dg.S + tid * kD64Ld);
 #pragma unroll
@@ -670,24 +605,11 @@ __global__ void __launch_bounds__(kSThreads, 1)
     }
     umma::fence_before_sync();
     __syncthreads();
-    int bad = diag64_factor(dg);
-    if (guard && upd && !fp && bad != kDiagTimeout) {
-      if (warp == 0) {
-        const bool f = guard_pivots_fail(dg.S, kD64Ld, Ab + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k),
-                                         tid & 31);
-        if ((tid & 31) == 0) *gfail = f ? 1 : 0;
-      }
-      __syncthreads();
-      fp = *gfail != 0;
-      __syncthreads();
-      if (fp) {
-        if (tid == 0) gstate[b] = k;
-        for (int h = 0; h < 2; ++h)
-          guard_tile_p<kSThreads>(L, Ab, n, k0, k0, 64, tid, 32 * h, nullptr, 0, dg.S, kD64Ld, gstage, tid,
-                                  CtaBarrier());
-        __syncthreads();
-        bad = diag64_factor(dg);
-      }
+    const int bad = diag64_factor(dg);
+    if (guard && upd && g == 0 && warp == 0 && bad != kDiagTimeout && gstate[b] < 0 &&
+        guard_pivots_fail(dg.S, kD64Ld, a + (size_t)b * n2 + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k),
+                          tid & 31)) {
+      if ((tid & 31) == 0) gstate[b] = k;
     }
     if (g == 0) {
       for (int e = tid; e < 64 * 16; e += kSThreads) {
@@ -721,16 +643,12 @@ __global__ void __launch_bounds__(kSThreads, 1)
     }
     // 3. Panel rows: X L_kk^T = P, one row (and one TMEM lane) per thread.
     for (int q = g; q < chunks; q += G) {
-      if (upd && !fp && q != g && !newest_panel(q, false)) {
+      if (upd && q != g && !newest_panel(q, false)) {
         ok = false;
         if (tid == 0 && info != nullptr) info[b] = -1;
         break;
       }
       const int r = k0 + 64 + q * kSThreads + tid;
-      if (fp) {
-        split_guard_rows<MODE>(L, Ab, n, k0, r, dg, gstage, W0, W1, tid);
-        continue;
-      }
       float d0[32], d1[32];
       if (upd) {
         umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 64u, d0);
@@ -801,14 +719,14 @@ static_assert(64 * kWideCols % kXCols == 0, "outer blocks are whole wide tiles")
 // Panel copies, then two per-matrix FP32 panel buffers (n x 64 each; block
 // columns alternate between them), then for large orders two per-matrix
 // outer-block buffers (n x 512 each, alternating by outer block), then the
-// pivot guard's per-matrix state (int32).
+// pivot guard's area.
 static size_t split_guard_offset(int64_t batch, int64_t n) {
   size_t bytes = (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 2 * (size_t)batch * n * 64 * sizeof(float);
   if (n >= kWideMinN) bytes += 2 * (size_t)batch * n * 64 * kWideCols * sizeof(float);
   return bytes;
 }
 size_t split_workspace_bytes(int64_t batch, int64_t n) {
-  return split_guard_offset(batch, n) + (((size_t)batch * sizeof(int32_t) + 255) & ~(size_t)255) + 1024;
+  return split_guard_offset(batch, n) + guard_ws_bytes(batch) + 1024;
 }
 
 namespace {
@@ -888,7 +806,9 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   pb[1] = pb[0] + (size_t)batch * n * 64;
   const int64_t sms = device_sms();
   const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(copies + split_guard_offset(batch, n));
+  uint8_t* garea = copies + split_guard_offset(batch, n);
+  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
+  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
   if (guard) {
     const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
@@ -1054,7 +974,8 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       if (int st = check(cudaEventRecord(side->join[k & 1], side->stream), "cudaEventRecord")) return st;
     }
   }
-  return B2P_OK;
+  // Every side-stream kernel has been joined into s by the last step.
+  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
 }
 
 }  // namespace b2p
