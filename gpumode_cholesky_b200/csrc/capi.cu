@@ -112,6 +112,13 @@ int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int pat
   }
 }
 
+// Whether a call on `path` runs the pivot guard (and so its rescue).
+static bool guarded(int path, int mode) {
+  const int m = mode & B2P_MODE_MASK;
+  return (mode & B2P_FLAG_GUARD) && (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3) &&
+         (path == B2P_PATH_FUSED || path == B2P_PATH_FUSED_WS || path == B2P_PATH_SPLIT);
+}
+
 static int check_mode(int mode) {
   const int m = mode & B2P_MODE_MASK;
   if (m > B2P_MODE_FP8 || (mode & ~(B2P_MODE_MASK | B2P_FLAG_FP64_DIAG | B2P_FLAG_GUARD)) != 0)
@@ -149,7 +156,7 @@ size_t b2p_potrf_path_workspace_size(int64_t batch, int64_t n, int mode, int pat
   if (batch <= 0 || n <= 128 || check_mode(mode) != B2P_OK) return 0;
   if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
   if (!path_supported(path, batch, n, mode)) return 0;
-  return path_workspace_bytes(path, batch, n, mode);
+  return path_workspace_bytes(path, batch, n, mode) + (guarded(path, mode) ? guard_ws_bytes(batch) : 0);
 }
 
 int b2p_potrf_batched(const float* a, float* l, int64_t batch, int64_t n, int mode,
@@ -177,17 +184,35 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
   const char* pl = reinterpret_cast<const char*>(l);
   if (pa < pl + bytes && pl < pa + bytes) return set_error(B2P_ERR_INVALID_ARG, "input and output overlap");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (fp32_from != nullptr) {
-    // -1 everywhere; the guarded kernels overwrite the matrices they touch.
-    const cudaError_t e = cudaMemsetAsync(fp32_from, 0xff, (size_t)batch * sizeof(int32_t), s);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(fp32_from): %s", cudaGetErrorString(e));
+  const bool auto_path = path == B2P_PATH_AUTO;
+  if (n > 128 && path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
+  const bool guard = n > 128 && guarded(path, mode);
+  // The guarded paths' state (first failing block column per matrix, -1
+  // for none: the caller's fp32_from when given) and the rescue's barrier
+  // words sit ahead of the path's own workspace.
+  int32_t* gstate = nullptr;
+  int* gbar = nullptr;
+  if (guard) {
+    const size_t gb = guard_ws_bytes(batch);
+    if (workspace == nullptr || workspace_bytes < gb)
+      return set_error(B2P_ERR_WORKSPACE, "workspace of at least %zu bytes required, %zu given", gb, workspace_bytes);
+    gstate = fp32_from ? fp32_from : static_cast<int32_t*>(workspace);
+    gbar = reinterpret_cast<int*>(static_cast<uint8_t*>(workspace) + gb - 256);
+    workspace = static_cast<uint8_t*>(workspace) + gb;
+    workspace_bytes -= gb;
+  }
+  if (fp32_from != nullptr || guard) {
+    // -1 everywhere; the guarded kernels record the matrices that trip.
+    int32_t* st = gstate ? gstate : fp32_from;
+    const cudaError_t e = cudaMemsetAsync(st, 0xff, (size_t)batch * sizeof(int32_t), s);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
   }
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);
-  const bool auto_path = path == B2P_PATH_AUTO;
-  if (path == B2P_PATH_AUTO) path = choose_path(batch, n, mode);
   if (!path_supported(path, batch, n, mode))
     return set_error(B2P_ERR_UNSUPPORTED, "path %d does not support n=%lld mode 0x%x", path, (long long)n, mode);
+  int st = B2P_OK;
+  bool done = false;
   if (auto_path && path == B2P_PATH_FUSED) {
     // One CTA per matrix runs in waves of `per` matrices; when the last wave
     // would be less than half full, those matrices run instead as clusters
@@ -196,15 +221,21 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
     const int64_t tail = batch % per;
     if (batch > per && tail > 0 && tail * 2 <= per && fused_ws_supported(tail, n, mode)) {
       const int64_t head = batch - tail;
-      if (int st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, fp32_from)) return st;
-      const size_t moff = (size_t)head * (size_t)n * (size_t)n;
-      const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
-      return potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
+      st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, gstate);
+      if (st == B2P_OK) {
+        const size_t moff = (size_t)head * (size_t)n * (size_t)n;
+        const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
+        st = potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
                             workspace_bytes - woff, info ? info + head : nullptr, s,
-                            fp32_from ? fp32_from + head : nullptr);
+                            gstate ? gstate + head : nullptr);
+      }
+      done = true;
     }
   }
-  return potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, fp32_from);
+  if (!done) st = potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, gstate);
+  if (st != B2P_OK || !guard) return st;
+  // Refactor in FP32 every matrix whose pivots the guard rejected.
+  return guard_rescue(a, l, batch, (int)n, gstate, gbar, info, s);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

@@ -53,20 +53,16 @@ __device__ __forceinline__ float guard_tau(int k) {
 }
 
 // True when some pivot of the factored diagonal block (dg_s: L_kk, row stride
-// ld, w valid rows) fails the threshold against A's diagonal (a_diag: the
-// element A[k0][k0], diagonal stride n + 1).  Called by one full warp.
-__device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, const float* a_diag, int64_t n, int w,
-                                                  float tau, int lane) {
+// ld) fails the threshold against A's diagonal (a_diag[j] = A[k0+j][k0+j],
+// staged in shared memory by the caller).  Called by one full warp.
+__device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, const float* a_diag, float tau,
+                                                  int lane) {
   bool fail = false;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int j = lane + 32 * h;
-    if (j < w) {
-      const float ljj = dg_s[j * ld + j];
-      const float d = ljj * ljj;
-      const float ajj = __ldg(a_diag + (size_t)j * (n + 1));
-      if (!(d > tau * ajj)) fail = true;  // also catches NaN and non-positive pivots
-    }
+    const float ljj = dg_s[j * ld + j];
+    if (!(ljj * ljj > tau * a_diag[j])) fail = true;  // also catches NaN and non-positive pivots
   }
   return __any_sync(0xffffffffu, fail);
 }

@@ -23,9 +23,9 @@
 // All mbarrier waits are bounded; a timeout marks the matrix with info = -1.
 //
 // With the pivot guard (guard.cuh) warp 0 checks the diagonal block's pivots
-// once it is factored and records the first failing column of the matrix;
-// the call then runs the FP32 rescue (potrf_rescue.cu) for the matrices
-// that tripped.
+// once it is factored (A's diagonal is staged in shared memory while P is
+// formed) and records the first failing column of the matrix; the caller
+// then runs the FP32 rescue (potrf_rescue.cu) for the matrices that tripped.
 //
 // The reference's left-looking paths run the same schedule through cuBLAS
 // and cuSOLVER (submission.py:3319-3409 _left_looking_large, 3606-3676,
@@ -59,7 +59,8 @@ constexpr uint32_t kFPhase2 = kFPtOff + 64 * kFPtLd * 4;
 constexpr uint32_t kFUnion = kFStaging > kFPhase2 ? kFStaging : kFPhase2;
 constexpr uint32_t kFZeroOff = kFUnion + 128;  // zeros, source of the strip's bulk stores
 constexpr uint32_t kFZeroBytes = 4096;           // >= 4 (n - 64) bytes for n <= 1024
-constexpr uint32_t kFSmemBytes = kFZeroOff + kFZeroBytes + 1024;
+constexpr uint32_t kFADiagOff = kFZeroOff + kFZeroBytes;  // A's diagonal of the current block (guard)
+constexpr uint32_t kFSmemBytes = kFADiagOff + 256 + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
 
 template <int MODE>
@@ -77,6 +78,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kFUnion + 48);
   int* flag = reinterpret_cast<int*>(sm + kFUnion + 56);
   int* badp = flag + 1;
+  float* adiag = reinterpret_cast<float*>(sm + kFADiagOff);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kFB;
@@ -229,6 +231,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
           if (mt == 0 && rl < 64) {
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
+            // A_jj for the guard (just loaded above, an L1 hit).
+            if (guard && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         umma::fence_before_sync();
@@ -241,7 +245,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
             break;
           }
           if (guard && k > 0 && warp == 0 && !tripped &&
-              guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane)) {
+              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane)) {
             tripped = true;
             if (lane == 0) gstate[b] = k;
           }
@@ -302,10 +306,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
   if (warp == 0) umma::tmem_dealloc(tmem, tmem_cols);
 }
 
-// The panel copies, then the pivot guard's area; the workspace pointer is
-// rounded up to 1024 bytes inside, hence the slack.
+// The workspace pointer is rounded up to 1024 bytes inside, hence the slack.
 size_t fused_workspace_bytes(int64_t batch, int64_t n) {
-  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + guard_ws_bytes(batch) + 1024;
+  return (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 1024;
 }
 
 bool fused_supported(int64_t n, int mode) {
@@ -315,7 +318,7 @@ bool fused_supported(int64_t n, int mode) {
 }
 
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* fp32_from) {
+                int32_t* info, cudaStream_t s, int32_t* gstate) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -325,14 +328,7 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const size_t smem = two ? kFSmemBytes : std::max<size_t>(kFSmemBytes, kFSmemOneCta);
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
-  const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  uint8_t* garea = wsa + (size_t)batch * 2 * panel_copy_region_bytes(n);
-  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
-  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
-  if (guard) {
-    const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
-  }
+  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
   {
     TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
     if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
@@ -345,8 +341,7 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
           <<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, gstate);
     }
   }
-  if (int st = check_launch("potrf_fused_kernel")) return st;
-  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
+  return check_launch("potrf_fused_kernel");
 }
 
 }  // namespace b2p

@@ -32,8 +32,9 @@
 // before TMEM is released.
 //
 // With the pivot guard (guard.cuh) warp 0 of rank 0 checks the diagonal
-// block's pivots and records the first failing column of the matrix; the
-// call then runs the FP32 rescue (potrf_rescue.cu) for those matrices.
+// block's pivots (A's diagonal is staged in shared memory while P is formed)
+// and records the first failing column of the matrix; the caller then runs
+// the FP32 rescue (potrf_rescue.cu) for those matrices.
 //
 // The reference's left-looking paths (submission.py:3319-3409, 3606-3676,
 // 5152-5196) issue the same three phases as separate cuSOLVER / cuBLAS /
@@ -67,7 +68,8 @@ constexpr uint32_t kWBarOff = kWZeroOff + kWZeroBytes;
 constexpr uint32_t kWCntOff = kWBarOff + 256;  // per-tile completion counters
 constexpr int kWMaxTiles = 64;                  // row tiles of a block column (n <= 8192)
 constexpr int kWMaxSlots = 8;                   // TMEM accumulator slots (512 columns)
-constexpr uint32_t kWSmemBytes = kWCntOff + 4 * kWMaxTiles + 1024;
+constexpr uint32_t kWADiagOff = kWCntOff + 4 * kWMaxTiles;  // A's diagonal of the current block (guard)
+constexpr uint32_t kWSmemBytes = kWADiagOff + 256 + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
 
@@ -244,6 +246,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
   const float* zeros = reinterpret_cast<const float*>(sm + kWZeroOff);
+  float* adiag = reinterpret_cast<float*>(sm + kWADiagOff);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
@@ -314,6 +317,8 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           if (mt == 0 && rl < 64) {
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
+            // A_jj for the guard (just loaded above, an L1 hit).
+            if (guard && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         cbar();
@@ -325,7 +330,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
           if (guard && k > 0 && rank == 0 && warp == 0 && !tripped && bad != kDiagTimeout &&
-              guard_pivots_fail(dg.S, kD64Ld, A + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k), lane)) {
+              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane)) {
             tripped = true;
             if (lane == 0) gstate[b] = k;
           }
@@ -474,7 +479,7 @@ bool fused_ws_fits(int64_t batch, int64_t n, int mode) {
 bool fused_ws_supported(int64_t batch, int64_t n, int mode) { return n <= 1024 && fused_ws_fits(batch, n, mode); }
 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                   int32_t* info, cudaStream_t s, int32_t* fp32_from) {
+                   int32_t* info, cudaStream_t s, int32_t* gstate) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -506,20 +511,11 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  uint8_t* garea = wsa + (size_t)batch * 2 * panel_copy_region_bytes(n);
-  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
-  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
-  if (guard) {
-    const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
-  }
-  {
-    TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, guard, gstate);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
-  }
-  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
+  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
+  TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, guard, gstate);
+  if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
+  return B2P_OK;
 }
 
 }  // namespace b2p

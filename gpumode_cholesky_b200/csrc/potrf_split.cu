@@ -476,7 +476,8 @@ constexpr uint32_t kSZero = 81920;     // zeros for the strip's bulk stores
 constexpr uint32_t kSZeroBytes = 4096;
 constexpr uint32_t kSDiag = kSZero + kSZeroBytes;
 constexpr uint32_t kSBar = kSDiag + (((uint32_t)sizeof(Diag64Smem) + 127u) & ~127u);
-constexpr uint32_t kSSmemBytes = kSBar + 64 + 1024;
+constexpr uint32_t kSADiag = kSBar + 64;  // A's diagonal of the current block (guard)
+constexpr uint32_t kSSmemBytes = kSADiag + 256 + 1024;
 constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the CTA's rows
 
 // Column k of every matrix, G CTAs per matrix.  P = base - X_{k-1} X_{k-1,kk}^T
@@ -488,8 +489,10 @@ constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the
 //
 // With the pivot guard (guard.cuh), warp 0 of the matrix's first CTA (g = 0)
 // checks the factored diagonal block, unless an earlier step has already
-// recorded a column for the matrix, and records k on a failure; the call
-// runs the FP32 rescue (potrf_rescue.cu) after its last step.
+// recorded a column for the matrix, and records k on a failure (A's
+// diagonal is loaded before the newest panel's product, so its latency is
+// hidden); the caller runs the FP32 rescue (potrf_rescue.cu) after the last
+// step.
 template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
@@ -502,6 +505,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
   uint64_t* done = full + 1;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSBar + 16);
   int* flag = reinterpret_cast<int*>(sm + kSBar + 24);
+  float* adiag = reinterpret_cast<float*>(sm + kSADiag);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int N = n / 64, k0 = 64 * k;
   const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
@@ -537,6 +541,14 @@ __global__ void __launch_bounds__(kSThreads, 1)
     uint8_t* W1 = W0 + rbytes;
     const float* base = (k >= 2) ? pbuf + (size_t)b * n * 64 : a + (size_t)b * n2 + k0;
     const size_t bld = (k >= 2) ? 64 : (size_t)n;
+    // Guard: this CTA checks the block unless the matrix has tripped already.
+    const bool gchk = guard && upd && g == 0 && gstate[b] < 0;
+    float ad0 = 0.f, ad1 = 0.f;
+    if (gchk && warp == 0) {
+      const float* ad = a + (size_t)b * n2 + (size_t)k0 * (n + 1);
+      ad0 = __ldg(ad + (size_t)(tid & 31) * (n + 1));
+      ad1 = __ldg(ad + (size_t)((tid & 31) + 32) * (n + 1));
+    }
 
     // The newest panel's product for the diagonal rows and chunk q (or the
     // diagonal rows only when q is out of range); false on a timeout.
@@ -603,12 +615,15 @@ __global__ void __launch_bounds__(kSThreads, 1)
         }
       }
     }
+    if (gchk && warp == 0) {
+      adiag[tid & 31] = ad0;
+      adiag[(tid & 31) + 32] = ad1;
+    }
     umma::fence_before_sync();
     __syncthreads();
     const int bad = diag64_factor(dg);
-    if (guard && upd && g == 0 && warp == 0 && bad != kDiagTimeout && gstate[b] < 0 &&
-        guard_pivots_fail(dg.S, kD64Ld, a + (size_t)b * n2 + (size_t)k0 * n + k0, n, 64, guard_tau<MODE>(k),
-                          tid & 31)) {
+    if (gchk && warp == 0 && bad != kDiagTimeout &&
+        guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), tid & 31)) {
       if ((tid & 31) == 0) gstate[b] = k;
     }
     if (g == 0) {
@@ -718,15 +733,11 @@ static_assert(64 * kWideCols % kXCols == 0, "outer blocks are whole wide tiles")
 
 // Panel copies, then two per-matrix FP32 panel buffers (n x 64 each; block
 // columns alternate between them), then for large orders two per-matrix
-// outer-block buffers (n x 512 each, alternating by outer block), then the
-// pivot guard's area.
-static size_t split_guard_offset(int64_t batch, int64_t n) {
+// outer-block buffers (n x 512 each, alternating by outer block).
+size_t split_workspace_bytes(int64_t batch, int64_t n) {
   size_t bytes = (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 2 * (size_t)batch * n * 64 * sizeof(float);
   if (n >= kWideMinN) bytes += 2 * (size_t)batch * n * 64 * kWideCols * sizeof(float);
-  return bytes;
-}
-size_t split_workspace_bytes(int64_t batch, int64_t n) {
-  return split_guard_offset(batch, n) + guard_ws_bytes(batch) + 1024;
+  return bytes + 1024;
 }
 
 namespace {
@@ -794,7 +805,7 @@ int side_stream(SideStream** out) {
 // wide kernel keeps to a bounded number of SMs so that the steps, which
 // carry the critical path, always find free ones.
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* fp32_from) {
+                int32_t* info, cudaStream_t s, int32_t* gstate) {
   const size_t need = split_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -805,14 +816,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   pb[0] = reinterpret_cast<float*>(copies + (size_t)batch * 2 * panel_copy_region_bytes(n));
   pb[1] = pb[0] + (size_t)batch * n * 64;
   const int64_t sms = device_sms();
-  const int guard = (mode & B2P_FLAG_GUARD) ? 1 : 0;
-  uint8_t* garea = copies + split_guard_offset(batch, n);
-  int32_t* gstate = fp32_from ? fp32_from : reinterpret_cast<int32_t*>(garea);
-  int* gbar = reinterpret_cast<int*>(garea + guard_ws_bytes(batch) - 256);
-  if (guard) {
-    const cudaError_t e = cudaMemsetAsync(gstate, 0xff, (size_t)batch * sizeof(int32_t), s);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
-  }
+  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
   auto upd = tf32 ? split_update_kernel<B2P_MODE_TF32> : split_update_kernel<B2P_MODE_BF16X3>;
   auto stp = tf32 ? split_step_kernel<B2P_MODE_TF32> : split_step_kernel<B2P_MODE_BF16X3>;
@@ -974,8 +978,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       if (int st = check(cudaEventRecord(side->join[k & 1], side->stream), "cudaEventRecord")) return st;
     }
   }
-  // Every side-stream kernel has been joined into s by the last step.
-  return guard ? guard_rescue(a, l, batch, n, gstate, gbar, info, s) : B2P_OK;
+  return B2P_OK;
 }
 
 }  // namespace b2p
