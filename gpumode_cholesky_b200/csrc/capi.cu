@@ -201,11 +201,10 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
     workspace = static_cast<uint8_t*>(workspace) + gb;
     workspace_bytes -= gb;
   }
-  if (fp32_from != nullptr || guard) {
-    // -1 everywhere; the guarded kernels record the matrices that trip.
-    int32_t* st = gstate ? gstate : fp32_from;
-    const cudaError_t e = cudaMemsetAsync(st, 0xff, (size_t)batch * sizeof(int32_t), s);
-    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(guard state): %s", cudaGetErrorString(e));
+  if (fp32_from != nullptr && !guard) {
+    // -1 everywhere (the guarded kernels write every matrix's entry themselves).
+    const cudaError_t e = cudaMemsetAsync(fp32_from, 0xff, (size_t)batch * sizeof(int32_t), s);
+    if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(fp32_from): %s", cudaGetErrorString(e));
   }
   if (n <= 32) return launch_warp32(a, l, dense_list(batch, (int)n), info, s);
   if (n <= 128) return launch_cta128(a, l, dense_list(batch, (int)n), info, s);

@@ -68,8 +68,10 @@ __device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, con
 }
 
 // FP32 update of one row against 32 columns of block column k, computed on
-// the SIMT cores: d[q] = sum_{j < k0} L[row][j] * L[k0 + c0 + q][j] (in order
-// of increasing j, fused multiply-adds).  L is read through L2 only: other
+// the SIMT cores: d[q] = sum_{j < k0} L[row][j] * L[k0 + c0 + q][j], each
+// 32-wide piece of j summed on its own (fused multiply-adds in order of j)
+// and added to d, so that no rounding chain runs over more than 32 + k0/32
+// additions.  L is read through L2 only: other
 // CTAs of the same launch write it.  Collective over the NT threads
 // that call it (barrier functor `bar`): each passes its own row (-1 for
 // none; d is then 0) and c0 (0 or 32, uniform within a warp); `stage` holds
@@ -101,7 +103,7 @@ __device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
         const float4* b = reinterpret_cast<const float4*>(stage + (c0 + q) * kGuardStageLd);
-        float s = d[q];
+        float s = 0.0f;
 #pragma unroll
         for (int j4 = 0; j4 < 8; ++j4) {
           const float4 v = b[j4];
@@ -110,7 +112,7 @@ __device__ __forceinline__ void guard_update_row(float (&d)[32], const float* __
           s = fmaf(x[4 * j4 + 2], v.z, s);
           s = fmaf(x[4 * j4 + 3], v.w, s);
         }
-        d[q] = s;
+        d[q] += s;
       }
     }
   }

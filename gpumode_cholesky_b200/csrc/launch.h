@@ -41,8 +41,8 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
 bool fused_supported(int64_t n, int mode);
 size_t fused_workspace_bytes(int64_t batch, int64_t n);
 // gstate (optional, device int32[batch]): with B2P_FLAG_GUARD, the kernels
-// write the first block column whose pivots fail the guard into gstate[b]
-// (the caller has set it to -1 and runs guard_rescue afterwards).
+// write into gstate[b] the first block column whose pivots fail the guard,
+// or -1, for every matrix (the caller runs guard_rescue afterwards).
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
                 int32_t* info, cudaStream_t s, int32_t* gstate = nullptr);
 // Warp-specialized variant (potrf_fused_ws.cu), in clusters of up to 8 CTAs
@@ -202,6 +202,18 @@ enum SmemSlot {
   kSlotTrsv1,
   kSlotGpForward,
   kSlotRescue,
+  kSlotFusedG0,
+  kSlotFusedG1,
+  kSlotFusedWsG0,
+  kSlotFusedWsG1,
+  kSlotFusedWsG2,
+  kSlotFusedWsG3,
+  kSlotFusedWsG4,
+  kSlotFusedWsG5,
+  kSlotFusedWsG6,
+  kSlotFusedWsG7,
+  kSlotSplitSG0,
+  kSlotSplitSG1,
   kSlotCount
 };
 

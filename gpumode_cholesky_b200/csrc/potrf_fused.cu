@@ -22,10 +22,11 @@
 // re-read and re-written through HBM, and the update accumulates in TMEM.
 // All mbarrier waits are bounded; a timeout marks the matrix with info = -1.
 //
-// With the pivot guard (guard.cuh) warp 0 checks the diagonal block's pivots
-// once it is factored (A's diagonal is staged in shared memory while P is
-// formed) and records the first failing column of the matrix; the caller
-// then runs the FP32 rescue (potrf_rescue.cu) for the matrices that tripped.
+// With the pivot guard (GUARD; guard.cuh) warp 0 checks the diagonal block's
+// pivots once it is factored (A's diagonal is staged in shared memory while
+// P is formed) and writes the first failing column of each matrix (or -1)
+// to gstate; the caller then runs the FP32 rescue (potrf_rescue.cu) for the
+// matrices that tripped.  The unguarded kernels are compiled without it.
 //
 // The reference's left-looking paths run the same schedule through cuBLAS
 // and cuSOLVER (submission.py:3319-3409 _left_looking_large, 3606-3676,
@@ -63,10 +64,10 @@ constexpr uint32_t kFADiagOff = kFZeroOff + kFZeroBytes;  // A's diagonal of the
 constexpr uint32_t kFSmemBytes = kFADiagOff + 256 + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
 
-template <int MODE>
+template <int MODE, bool GUARD>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info, int guard,
+                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info,
                        int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *badp = -1;
-    bool tripped = false;  // warp 0: the guard has recorded a column of this matrix
+    int trip = -1;  // warp 0: the first block column whose pivots the guard rejected
 
     for (int k = 0; k < N; ++k) {
       const int k0 = k * kFB;
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
             // A_jj for the guard (just loaded above, an L1 hit).
-            if (guard && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
+            if (GUARD && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         umma::fence_before_sync();
@@ -244,11 +245,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
             ok = false;
             break;
           }
-          if (guard && k > 0 && warp == 0 && !tripped &&
-              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane)) {
-            tripped = true;
-            if (lane == 0) gstate[b] = k;
-          }
+          if (GUARD && k > 0 && warp == 0 && trip < 0 &&
+              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane))
+            trip = k;
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
           for (int e = tid; e < 64 * 16; e += kFThreads) {
@@ -294,6 +293,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
       umma::fence_after_sync();
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
+    if (GUARD && tid == 0) gstate[b] = trip;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
@@ -328,18 +328,18 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const size_t smem = two ? kFSmemBytes : std::max<size_t>(kFSmemBytes, kFSmemOneCta);
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
-  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
+  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
+  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
+  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, uint32_t, int32_t*, int32_t*);
+  static const Kern kernels[2][2] = {
+      {potrf_fused_kernel<B2P_MODE_TF32, false>, potrf_fused_kernel<B2P_MODE_TF32, true>},
+      {potrf_fused_kernel<B2P_MODE_BF16X3, false>, potrf_fused_kernel<B2P_MODE_BF16X3, true>}};
+  const Kern kern = kernels[tf32 ? 0 : 1][guard ? 1 : 0];
+  const int slot = guard ? (tf32 ? kSlotFusedG0 : kSlotFusedG1) : (tf32 ? kSlotFused0 : kSlotFused1);
+  if (int st = ensure_smem_attr((const void*)kern, smem, slot)) return st;
   {
     TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
-    if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
-      if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
-      potrf_fused_kernel<B2P_MODE_TF32>
-          <<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, gstate);
-    } else {
-      if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
-      potrf_fused_kernel<B2P_MODE_BF16X3>
-          <<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, guard, gstate);
-    }
+    kern<<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, gstate);
   }
   return check_launch("potrf_fused_kernel");
 }

@@ -31,10 +31,11 @@
 // marks the matrix with info = -1 and drains outstanding copies and MMAs
 // before TMEM is released.
 //
-// With the pivot guard (guard.cuh) warp 0 of rank 0 checks the diagonal
-// block's pivots (A's diagonal is staged in shared memory while P is formed)
-// and records the first failing column of the matrix; the caller then runs
-// the FP32 rescue (potrf_rescue.cu) for those matrices.
+// With the pivot guard (GUARD; guard.cuh) warp 0 of rank 0 checks the
+// diagonal block's pivots (A's diagonal is staged in shared memory while P
+// is formed) and writes the first failing column of each matrix (or -1) to
+// gstate; the caller then runs the FP32 rescue (potrf_rescue.cu) for those
+// matrices.  The unguarded kernels are compiled without it.
 //
 // The reference's left-looking paths (submission.py:3319-3409, 3606-3676,
 // 5152-5196) issue the same three phases as separate cuSOLVER / cuBLAS /
@@ -239,9 +240,9 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
 
 // ---------------------------------------------------------------------------
 // Consumers: warps 0-7.
-template <int MODE, int CL>
+template <int MODE, int CL, bool GUARD>
 __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
-                             int n, uint32_t tmem, int32_t* info, int rank, int guard, int32_t* gstate) {
+                             int n, uint32_t tmem, int32_t* info, int rank, int32_t* gstate) {
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
@@ -259,7 +260,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *br.badp = -1;
     bool failed = false;
-    bool tripped = false;  // warp 0: the guard has recorded a column of this matrix
+    int trip = -1;  // warp 0: the first block column whose pivots the guard rejected
     for (int k = 0; k < N && !failed; ++k) {
       const int k0 = k * kWB;
       const int mt_n = (n - k0 + kWM - 1) / kWM;
@@ -318,7 +319,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
             // A_jj for the guard (just loaded above, an L1 hit).
-            if (guard && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
+            if (GUARD && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         cbar();
@@ -329,11 +330,9 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             failed = true;
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
-          if (guard && k > 0 && rank == 0 && warp == 0 && !tripped && bad != kDiagTimeout &&
-              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane)) {
-            tripped = true;
-            if (lane == 0) gstate[b] = k;
-          }
+          if (GUARD && k > 0 && rank == 0 && warp == 0 && trip < 0 && bad != kDiagTimeout &&
+              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane))
+            trip = k;
           if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
           for (int e = tid; e < (rank == 0 ? 64 * 16 : 0); e += kWConsumers) {
             const int r = e >> 4, c = (e & 15) * 4;
@@ -390,17 +389,17 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
       }
     }
     if (tid == 0 && rank == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
+    if (GUARD && tid == 0 && rank == 0) gstate[b] = trip;
     if (failed) break;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
 }
 
-template <int MODE, int CL>
+template <int MODE, int CL, bool GUARD>
 __global__ void __launch_bounds__(kWThreads, 1)
     potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                          uint8_t* __restrict__ ws, int32_t* __restrict__ info, int guard,
-                          int32_t* __restrict__ gstate) {
+                          uint8_t* __restrict__ ws, int32_t* __restrict__ info, int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char wraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wraw) + 1023) & ~(uintptr_t)1023);
   WsBars br;
@@ -442,7 +441,7 @@ __global__ void __launch_bounds__(kWThreads, 1)
   if (warp == kWConsumers / 32) {
     if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
-    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank, guard, gstate);
+    ws_consumers<MODE, CL, GUARD>(br, sm, a, l, ws, batch, n, tmem, info, rank, gstate);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -490,15 +489,21 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
     return set_error(B2P_ERR_UNSUPPORTED, "warp-specialized path: n=%d not supported", n);
   const int grid = cl * (int)std::max<int64_t>(1, std::min<int64_t>(batch, sms / cl));
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*, int, int32_t*);
-  static const Kern kernels[2][4] = {
-      {potrf_fused_ws_kernel<B2P_MODE_TF32, 1>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2>,
-       potrf_fused_ws_kernel<B2P_MODE_TF32, 4>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8>},
-      {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2>,
-       potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8>}};
+  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
+  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*, int32_t*);
+  static const Kern kernels[2][2][4] = {
+      {{potrf_fused_ws_kernel<B2P_MODE_TF32, 1, false>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2, false>,
+        potrf_fused_ws_kernel<B2P_MODE_TF32, 4, false>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8, false>},
+       {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1, false>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2, false>,
+        potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4, false>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8, false>}},
+      {{potrf_fused_ws_kernel<B2P_MODE_TF32, 1, true>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2, true>,
+        potrf_fused_ws_kernel<B2P_MODE_TF32, 4, true>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8, true>},
+       {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1, true>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2, true>,
+        potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4, true>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8, true>}}};
   const int li = cl == 1 ? 0 : cl == 2 ? 1 : cl == 4 ? 2 : 3;
-  const Kern kern = kernels[tf32 ? 0 : 1][li];
-  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, kSlotFusedWs0 + (tf32 ? 0 : 4) + li)) return st;
+  const Kern kern = kernels[guard ? 1 : 0][tf32 ? 0 : 1][li];
+  const int slot = (guard ? kSlotFusedWsG0 : kSlotFusedWs0) + (tf32 ? 0 : 4) + li;
+  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, slot)) return st;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid, 1, 1);
   cfg.blockDim = dim3(kWThreads, 1, 1);
@@ -511,9 +516,8 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
   TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, guard, gstate);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, gstate);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }

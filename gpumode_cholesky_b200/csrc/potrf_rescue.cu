@@ -84,6 +84,11 @@ __global__ void __launch_bounds__(kRThreads, 1)
   const int N = n / 64;
   const size_t n2 = (size_t)n * n;
 
+  // Fast exit: nothing flagged (the usual case).
+  bool any = false;
+  for (int64_t b = tid; b < batch; b += kRThreads) any |= __ldcg(gstate + b) >= 0;
+  if (!__syncthreads_or(any)) return;
+
   int64_t scan = 0;
   while (scan < batch) {
     // Ordered compaction of the next flagged matrices into the list.

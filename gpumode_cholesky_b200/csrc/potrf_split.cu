@@ -487,17 +487,17 @@ constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the
 // the CTA's 128-row chunks by forward substitution (one row per thread,
 // which is also one TMEM lane per thread), write L and the panel copy.
 //
-// With the pivot guard (guard.cuh), warp 0 of the matrix's first CTA (g = 0)
-// checks the factored diagonal block, unless an earlier step has already
-// recorded a column for the matrix, and records k on a failure (A's
-// diagonal is loaded before the newest panel's product, so its latency is
-// hidden); the caller runs the FP32 rescue (potrf_rescue.cu) after the last
-// step.
-template <int MODE>
+// With the pivot guard (GUARD; guard.cuh), the matrix's first CTA (g = 0)
+// sets gstate[b] = -1 in step 0; in later steps its warp 0 checks the
+// factored diagonal block, unless an earlier step has already recorded a
+// column for the matrix, and records k on a failure (A's diagonal is loaded
+// before the newest panel's product, so its latency is hidden).  The caller
+// runs the FP32 rescue (potrf_rescue.cu) after the last step.
+template <int MODE, bool GUARD>
 __global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info, int guard, int32_t* __restrict__ gstate) {
+                      int32_t* __restrict__ info, int32_t* __restrict__ gstate) {
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -542,7 +542,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
     const float* base = (k >= 2) ? pbuf + (size_t)b * n * 64 : a + (size_t)b * n2 + k0;
     const size_t bld = (k >= 2) ? 64 : (size_t)n;
     // Guard: this CTA checks the block unless the matrix has tripped already.
-    const bool gchk = guard && upd && g == 0 && gstate[b] < 0;
+    if (GUARD && !upd && g == 0 && tid == 0) gstate[b] = -1;
+    const bool gchk = GUARD && upd && g == 0 && gstate[b] < 0;
     float ad0 = 0.f, ad1 = 0.f;
     if (gchk && warp == 0) {
       const float* ad = a + (size_t)b * n2 + (size_t)k0 * (n + 1);
@@ -816,13 +817,16 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   pb[0] = reinterpret_cast<float*>(copies + (size_t)batch * 2 * panel_copy_region_bytes(n));
   pb[1] = pb[0] + (size_t)batch * n * 64;
   const int64_t sms = device_sms();
-  const int guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr ? 1 : 0;
+  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
   auto upd = tf32 ? split_update_kernel<B2P_MODE_TF32> : split_update_kernel<B2P_MODE_BF16X3>;
-  auto stp = tf32 ? split_step_kernel<B2P_MODE_TF32> : split_step_kernel<B2P_MODE_BF16X3>;
+  auto stp = tf32 ? (guard ? split_step_kernel<B2P_MODE_TF32, true> : split_step_kernel<B2P_MODE_TF32, false>)
+                  : (guard ? split_step_kernel<B2P_MODE_BF16X3, true> : split_step_kernel<B2P_MODE_BF16X3, false>);
   auto wdk = tf32 ? split_wide_kernel<B2P_MODE_TF32> : split_wide_kernel<B2P_MODE_BF16X3>;
   if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, tf32 ? kSlotSplitU0 : kSlotSplitU1)) return st;
-  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, tf32 ? kSlotSplitS0 : kSlotSplitS1)) return st;
+  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes,
+                                guard ? (tf32 ? kSlotSplitSG0 : kSlotSplitSG1) : (tf32 ? kSlotSplitS0 : kSlotSplitS1)))
+    return st;
   const int N = n / 64;
   const int64_t n2 = (int64_t)n * n;
   const bool wide = n >= kWideMinN;
@@ -936,7 +940,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       TraceScope ts(kKSplitStep, s,
                     batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
       const cudaError_t e =
-          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, guard, gstate);
+          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, gstate);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,
