@@ -103,11 +103,11 @@ size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
 }
 
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
-               int32_t* info, cudaStream_t s, int32_t* fp32_from) {
+               int32_t* info, cudaStream_t s) {
   switch (path) {
-    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
-    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
-    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s, fp32_from);
+    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s);
+    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s);
     default: return potrf_blocked(a, l, batch, n, mode, ws, ws_bytes, info, s);
   }
 }
@@ -202,7 +202,7 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
     workspace_bytes -= gb;
   }
   if (fp32_from != nullptr && !guard) {
-    // -1 everywhere (the guarded kernels write every matrix's entry themselves).
+    // -1 everywhere (a guarded call's audit writes every matrix's entry).
     const cudaError_t e = cudaMemsetAsync(fp32_from, 0xff, (size_t)batch * sizeof(int32_t), s);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(fp32_from): %s", cudaGetErrorString(e));
   }
@@ -220,21 +220,20 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
     const int64_t tail = batch % per;
     if (batch > per && tail > 0 && tail * 2 <= per && fused_ws_supported(tail, n, mode)) {
       const int64_t head = batch - tail;
-      st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, gstate);
+      st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s);
       if (st == B2P_OK) {
         const size_t moff = (size_t)head * (size_t)n * (size_t)n;
         const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
         st = potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
-                            workspace_bytes - woff, info ? info + head : nullptr, s,
-                            gstate ? gstate + head : nullptr);
+                            workspace_bytes - woff, info ? info + head : nullptr, s);
       }
       done = true;
     }
   }
-  if (!done) st = potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, gstate);
+  if (!done) st = potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s);
   if (st != B2P_OK || !guard) return st;
-  // Refactor in FP32 every matrix whose pivots the guard rejected.
-  return guard_rescue(a, l, batch, (int)n, gstate, gbar, info, s);
+  // Audit the pivots and refactor in FP32 every matrix whose pivots fail.
+  return guard_rescue(a, l, batch, (int)n, mode, gstate, gbar, info, s);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

@@ -14,22 +14,25 @@
 // of a jitter term (Gaussian-process kernels) while the plain FP32 path
 // factors them.
 //
-// The guard therefore checks, after the diagonal block of column k is
-// factored, every pivot against
-//     d_j = L_jj^2  >  kGuardMargin * delta(k) * A_jj
-// (non-finite or non-positive pivots fail too) and records the first
-// failing column of each matrix.  A matrix that trips is then refactored
-// from its first column in FP32 on the SIMT cores (potrf_rescue.cu), in one
-// more launch that does nothing when no matrix tripped.  Recomputing only
-// from the failing column on is not enough: the mixed columns before it
-// already carry a backward error of about delta * |A|, which can exceed the
-// smallest eigenvalues of the remaining Schur complement (on the Gaussian-
-// process kernels of order 2048 an FP32 recompute from the failing column on
-// still met a negative pivot, while a restart from column 0 gave the FP32
-// residual).  The reference's closest analogue is the accurate retry of its
-// 256-order kernel, triggered when a pivot falls under 1e-2 of the input's
-// diagonal (submission.py:866-868, 883-886, 1004-1031), which likewise
-// refactors the whole matrix in FP32.
+// The guard therefore audits, once the tensor-mode path has factored the
+// batch, every computed pivot against
+//     d_j = L_jj^2  >  kGuardMargin * delta(k) * A_jj     (k = j / 64)
+// (non-finite or non-positive pivots fail too); a matrix's first failing
+// block column is its guard state.  The pivot L_jj stored by the path is
+// the one its own diagonal block produced, so the audit sees exactly what
+// a check inside the kernels would, at no cost to them.  A matrix that
+// fails is refactored from its first column in FP32 on the SIMT cores
+// (potrf_rescue.cu; the same launch does the audit and does nothing more
+// when no matrix fails).  Recomputing only from the failing column on is
+// not enough: the mixed columns before it already carry a backward error of
+// about delta * |A|, which can exceed the smallest eigenvalues of the
+// remaining Schur complement (on the Gaussian-process kernels of order 2048
+// an FP32 recompute from the failing column on still met a negative pivot,
+// while a restart from column 0 gave the FP32 residual).  The reference's
+// closest analogue is the accurate retry of its 256-order kernel, triggered
+// when a pivot falls under 1e-2 of the input's diagonal
+// (submission.py:866-868, 883-886, 1004-1031), which likewise refactors the
+// whole matrix in FP32.
 #pragma once
 
 #include <stdint.h>
@@ -42,29 +45,14 @@ constexpr float kGuardMargin = 2.0f;
 constexpr int kGuardStageLd = 36;  // floats per staged row of the FP32 update
 constexpr int kGuardStageFloats = 64 * kGuardStageLd;
 
-// Pivot threshold (relative to A_jj) for block column k (k0 = 64 k) of a
-// mode; 0 disables the check (no update before column 0).
-template <int MODE>
-__device__ __forceinline__ float guard_tau(int k) {
+// Pivot threshold (relative to A_jj) for block column k of a tensor mode;
+// 0 for column 0, which no update precedes.
+__device__ __forceinline__ float guard_tau(int mode, int k) {
   if (k == 0) return 0.0f;
-  constexpr float kRep = MODE == B2P_MODE_TF32 ? 9.765625e-4f : 1.52587890625e-5f;  // 2^-10, 2^-16
-  constexpr float kSteps = MODE == B2P_MODE_TF32 ? 8.0f : 12.0f;                      // MMAs per 64-wide chunk
-  return kGuardMargin * (kRep + kSteps * (float)k * 1.1920928955078125e-7f);         // 2^-23
-}
-
-// True when some pivot of the factored diagonal block (dg_s: L_kk, row stride
-// ld) fails the threshold against A's diagonal (a_diag[j] = A[k0+j][k0+j],
-// staged in shared memory by the caller).  Called by one full warp.
-__device__ __forceinline__ bool guard_pivots_fail(const float* dg_s, int ld, const float* a_diag, float tau,
-                                                  int lane) {
-  bool fail = false;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int j = lane + 32 * h;
-    const float ljj = dg_s[j * ld + j];
-    if (!(ljj * ljj > tau * a_diag[j])) fail = true;  // also catches NaN and non-positive pivots
-  }
-  return __any_sync(0xffffffffu, fail);
+  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
+  const float rep = tf32 ? 9.765625e-4f : 1.52587890625e-5f;  // 2^-10, 2^-16
+  const float steps = tf32 ? 8.0f : 12.0f;                     // MMAs per 64-wide chunk
+  return kGuardMargin * (rep + steps * (float)k * 1.1920928955078125e-7f);  // 2^-23 per step
 }
 
 // FP32 update of one row against 32 columns of block column k, computed on

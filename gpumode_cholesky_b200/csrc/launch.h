@@ -40,15 +40,12 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
 // Fused left-looking tensor-core path for 128 < n <= 1024, n % 64 == 0 (potrf_fused.cu).
 bool fused_supported(int64_t n, int mode);
 size_t fused_workspace_bytes(int64_t batch, int64_t n);
-// gstate (optional, device int32[batch]): with B2P_FLAG_GUARD, the kernels
-// write into gstate[b] the first block column whose pivots fail the guard,
-// or -1, for every matrix (the caller runs guard_rescue afterwards).
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* gstate = nullptr);
+                int32_t* info, cudaStream_t s);
 // Warp-specialized variant (potrf_fused_ws.cu), in clusters of up to 8 CTAs
 // per matrix for small batches: same workspace and contract.
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                   int32_t* info, cudaStream_t s, int32_t* gstate = nullptr);
+                   int32_t* info, cudaStream_t s);
 // Orders and batches the warp-specialized kernel can take (n <= 8192, in
 // clusters large enough for TMEM), and the subset the dispatcher and the
 // forced-path entry point offer (n <= 1024).
@@ -59,9 +56,10 @@ bool fused_ws_supported(int64_t batch, int64_t n, int mode);
 // its path's own workspace, guard_ws_bytes(batch): the per-matrix guard
 // state (int32: first failing block column, -1 for none; the caller's
 // fp32_from array takes its place when given) and two barrier words.
-// guard_rescue refactors in FP32 every matrix whose state is >= 0.
+// guard_rescue audits the pivots the tensor-mode path (mode) left in l and
+// refactors in FP32 every matrix whose pivots fail.
 size_t guard_ws_bytes(int64_t batch);
-int guard_rescue(const float* a, float* l, int64_t batch, int n, const int32_t* gstate, int* bar, int32_t* info,
+int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, int* bar, int32_t* info,
                  cudaStream_t s);
 
 // Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
@@ -69,7 +67,7 @@ int guard_rescue(const float* a, float* l, int64_t batch, int n, const int32_t* 
 bool split_supported(int64_t n, int mode);
 size_t split_workspace_bytes(int64_t batch, int64_t n);
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* gstate = nullptr);
+                int32_t* info, cudaStream_t s);
 
 // The n > 128 dispatcher (capi.cu): the path for (batch, n, mode), whether a
 // path takes a shape, its workspace, and a launch on an explicit path (n > 128;
@@ -78,7 +76,7 @@ int choose_path(int64_t batch, int64_t n, int mode);
 bool path_supported(int path, int64_t batch, int64_t n, int mode);
 size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode);
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
-               int32_t* info, cudaStream_t s, int32_t* gstate = nullptr);
+               int32_t* info, cudaStream_t s);
 
 // Batched triangular solves with L (trsv.cu): x = L^{-1} b, or L^{-T} b.
 constexpr int kTrsvMaxN = 32768;  // x is held in shared memory (n floats)
@@ -202,18 +200,6 @@ enum SmemSlot {
   kSlotTrsv1,
   kSlotGpForward,
   kSlotRescue,
-  kSlotFusedG0,
-  kSlotFusedG1,
-  kSlotFusedWsG0,
-  kSlotFusedWsG1,
-  kSlotFusedWsG2,
-  kSlotFusedWsG3,
-  kSlotFusedWsG4,
-  kSlotFusedWsG5,
-  kSlotFusedWsG6,
-  kSlotFusedWsG7,
-  kSlotSplitSG0,
-  kSlotSplitSG1,
   kSlotCount
 };
 

@@ -22,19 +22,12 @@
 // re-read and re-written through HBM, and the update accumulates in TMEM.
 // All mbarrier waits are bounded; a timeout marks the matrix with info = -1.
 //
-// With the pivot guard (GUARD; guard.cuh) warp 0 checks the diagonal block's
-// pivots once it is factored (A's diagonal is staged in shared memory while
-// P is formed) and writes the first failing column of each matrix (or -1)
-// to gstate; the caller then runs the FP32 rescue (potrf_rescue.cu) for the
-// matrices that tripped.  The unguarded kernels are compiled without it.
-//
 // The reference's left-looking paths run the same schedule through cuBLAS
 // and cuSOLVER (submission.py:3319-3409 _left_looking_large, 3606-3676,
 // 5152-5196 e62 with a resident diagonal block and inverse panel multiply).
 #include <algorithm>
 
 #include "diag64.cuh"
-#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -60,15 +53,13 @@ constexpr uint32_t kFPhase2 = kFPtOff + 64 * kFPtLd * 4;
 constexpr uint32_t kFUnion = kFStaging > kFPhase2 ? kFStaging : kFPhase2;
 constexpr uint32_t kFZeroOff = kFUnion + 128;  // zeros, source of the strip's bulk stores
 constexpr uint32_t kFZeroBytes = 4096;           // >= 4 (n - 64) bytes for n <= 1024
-constexpr uint32_t kFADiagOff = kFZeroOff + kFZeroBytes;  // A's diagonal of the current block (guard)
-constexpr uint32_t kFSmemBytes = kFADiagOff + 256 + 1024;
+constexpr uint32_t kFSmemBytes = kFZeroOff + kFZeroBytes + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
 
-template <int MODE, bool GUARD>
+template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info,
-                       int32_t* __restrict__ gstate) {
+                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info) {
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
@@ -79,7 +70,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kFUnion + 48);
   int* flag = reinterpret_cast<int*>(sm + kFUnion + 56);
   int* badp = flag + 1;
-  float* adiag = reinterpret_cast<float*>(sm + kFADiagOff);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kFB;
@@ -115,7 +105,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
     uint8_t* W0 = ws + (size_t)b * 2 * rbytes;
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *badp = -1;
-    int trip = -1;  // warp 0: the first block column whose pivots the guard rejected
 
     for (int k = 0; k < N; ++k) {
       const int k0 = k * kFB;
@@ -232,8 +221,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
           if (mt == 0 && rl < 64) {
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
-            // A_jj for the guard (just loaded above, an L1 hit).
-            if (GUARD && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         umma::fence_before_sync();
@@ -245,9 +232,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
             ok = false;
             break;
           }
-          if (GUARD && k > 0 && warp == 0 && trip < 0 &&
-              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane))
-            trip = k;
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
           for (int e = tid; e < 64 * 16; e += kFThreads) {
@@ -293,7 +277,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
       umma::fence_after_sync();
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
-    if (GUARD && tid == 0) gstate[b] = trip;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
@@ -318,7 +301,7 @@ bool fused_supported(int64_t n, int mode) {
 }
 
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* gstate) {
+                int32_t* info, cudaStream_t s) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -328,18 +311,13 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const size_t smem = two ? kFSmemBytes : std::max<size_t>(kFSmemBytes, kFSmemOneCta);
   const int sms = device_sms();
   const int grid = (int)std::min<int64_t>(batch, (int64_t)sms * (two ? 2 : 1));
-  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
-  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, uint32_t, int32_t*, int32_t*);
-  static const Kern kernels[2][2] = {
-      {potrf_fused_kernel<B2P_MODE_TF32, false>, potrf_fused_kernel<B2P_MODE_TF32, true>},
-      {potrf_fused_kernel<B2P_MODE_BF16X3, false>, potrf_fused_kernel<B2P_MODE_BF16X3, true>}};
-  const Kern kern = kernels[tf32 ? 0 : 1][guard ? 1 : 0];
-  const int slot = guard ? (tf32 ? kSlotFusedG0 : kSlotFusedG1) : (tf32 ? kSlotFused0 : kSlotFused1);
-  if (int st = ensure_smem_attr((const void*)kern, smem, slot)) return st;
-  {
-    TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
-    kern<<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, gstate);
+  TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
+  if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
+    if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
+    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
+  } else {
+    if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
+    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
   }
   return check_launch("potrf_fused_kernel");
 }

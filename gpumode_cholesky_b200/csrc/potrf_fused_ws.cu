@@ -31,19 +31,12 @@
 // marks the matrix with info = -1 and drains outstanding copies and MMAs
 // before TMEM is released.
 //
-// With the pivot guard (GUARD; guard.cuh) warp 0 of rank 0 checks the
-// diagonal block's pivots (A's diagonal is staged in shared memory while P
-// is formed) and writes the first failing column of each matrix (or -1) to
-// gstate; the caller then runs the FP32 rescue (potrf_rescue.cu) for those
-// matrices.  The unguarded kernels are compiled without it.
-//
 // The reference's left-looking paths (submission.py:3319-3409, 3606-3676,
 // 5152-5196) issue the same three phases as separate cuSOLVER / cuBLAS /
 // CUDA calls with host round trips between them.
 #include <algorithm>
 
 #include "diag64.cuh"
-#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -69,8 +62,7 @@ constexpr uint32_t kWBarOff = kWZeroOff + kWZeroBytes;
 constexpr uint32_t kWCntOff = kWBarOff + 256;  // per-tile completion counters
 constexpr int kWMaxTiles = 64;                  // row tiles of a block column (n <= 8192)
 constexpr int kWMaxSlots = 8;                   // TMEM accumulator slots (512 columns)
-constexpr uint32_t kWADiagOff = kWCntOff + 4 * kWMaxTiles;  // A's diagonal of the current block (guard)
-constexpr uint32_t kWSmemBytes = kWADiagOff + 256 + 1024;
+constexpr uint32_t kWSmemBytes = kWCntOff + 4 * kWMaxTiles + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
 
@@ -240,14 +232,13 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
 
 // ---------------------------------------------------------------------------
 // Consumers: warps 0-7.
-template <int MODE, int CL, bool GUARD>
+template <int MODE, int CL>
 __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
-                             int n, uint32_t tmem, int32_t* info, int rank, int32_t* gstate) {
+                             int n, uint32_t tmem, int32_t* info, int rank) {
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
   const float* zeros = reinterpret_cast<const float*>(sm + kWZeroOff);
-  float* adiag = reinterpret_cast<float*>(sm + kWADiagOff);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = n / kWB;
   const size_t rbytes = panel_copy_region_bytes(n);
@@ -260,7 +251,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
     uint8_t* W1 = W0 + rbytes;
     if (tid == 0) *br.badp = -1;
     bool failed = false;
-    int trip = -1;  // warp 0: the first block column whose pivots the guard rejected
     for (int k = 0; k < N && !failed; ++k) {
       const int k0 = k * kWB;
       const int mt_n = (n - k0 + kWM - 1) / kWM;
@@ -318,8 +308,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           if (mt == 0 && rl < 64) {
 #pragma unroll
             for (int q = 0; q < 32; ++q) dg.S[rl * kD64Ld + 32 * h + q] = p[q];
-            // A_jj for the guard (just loaded above, an L1 hit).
-            if (GUARD && (rl >> 5) == h) adiag[rl] = A[(size_t)(k0 + rl) * n + k0 + rl];
           }
         }
         cbar();
@@ -330,9 +318,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             failed = true;
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
-          if (GUARD && k > 0 && rank == 0 && warp == 0 && trip < 0 && bad != kDiagTimeout &&
-              guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), lane))
-            trip = k;
           if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
           for (int e = tid; e < (rank == 0 ? 64 * 16 : 0); e += kWConsumers) {
             const int r = e >> 4, c = (e & 15) * 4;
@@ -389,17 +374,16 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
       }
     }
     if (tid == 0 && rank == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
-    if (GUARD && tid == 0 && rank == 0) gstate[b] = trip;
     if (failed) break;
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == 0) umma::bulk_wait_all();
 }
 
-template <int MODE, int CL, bool GUARD>
+template <int MODE, int CL>
 __global__ void __launch_bounds__(kWThreads, 1)
     potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                          uint8_t* __restrict__ ws, int32_t* __restrict__ info, int32_t* __restrict__ gstate) {
+                          uint8_t* __restrict__ ws, int32_t* __restrict__ info) {
   extern __shared__ unsigned char wraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wraw) + 1023) & ~(uintptr_t)1023);
   WsBars br;
@@ -441,7 +425,7 @@ __global__ void __launch_bounds__(kWThreads, 1)
   if (warp == kWConsumers / 32) {
     if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
-    ws_consumers<MODE, CL, GUARD>(br, sm, a, l, ws, batch, n, tmem, info, rank, gstate);
+    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -478,7 +462,7 @@ bool fused_ws_fits(int64_t batch, int64_t n, int mode) {
 bool fused_ws_supported(int64_t batch, int64_t n, int mode) { return n <= 1024 && fused_ws_fits(batch, n, mode); }
 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                   int32_t* info, cudaStream_t s, int32_t* gstate) {
+                   int32_t* info, cudaStream_t s) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -489,21 +473,15 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
     return set_error(B2P_ERR_UNSUPPORTED, "warp-specialized path: n=%d not supported", n);
   const int grid = cl * (int)std::max<int64_t>(1, std::min<int64_t>(batch, sms / cl));
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
-  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*, int32_t*);
-  static const Kern kernels[2][2][4] = {
-      {{potrf_fused_ws_kernel<B2P_MODE_TF32, 1, false>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2, false>,
-        potrf_fused_ws_kernel<B2P_MODE_TF32, 4, false>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8, false>},
-       {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1, false>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2, false>,
-        potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4, false>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8, false>}},
-      {{potrf_fused_ws_kernel<B2P_MODE_TF32, 1, true>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2, true>,
-        potrf_fused_ws_kernel<B2P_MODE_TF32, 4, true>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8, true>},
-       {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1, true>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2, true>,
-        potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4, true>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8, true>}}};
+  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*);
+  static const Kern kernels[2][4] = {
+      {potrf_fused_ws_kernel<B2P_MODE_TF32, 1>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2>,
+       potrf_fused_ws_kernel<B2P_MODE_TF32, 4>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8>},
+      {potrf_fused_ws_kernel<B2P_MODE_BF16X3, 1>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 2>,
+       potrf_fused_ws_kernel<B2P_MODE_BF16X3, 4>, potrf_fused_ws_kernel<B2P_MODE_BF16X3, 8>}};
   const int li = cl == 1 ? 0 : cl == 2 ? 1 : cl == 4 ? 2 : 3;
-  const Kern kern = kernels[guard ? 1 : 0][tf32 ? 0 : 1][li];
-  const int slot = (guard ? kSlotFusedWsG0 : kSlotFusedWs0) + (tf32 ? 0 : 4) + li;
-  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, slot)) return st;
+  const Kern kern = kernels[tf32 ? 0 : 1][li];
+  if (int st = ensure_smem_attr((const void*)kern, kWSmemBytes, kSlotFusedWs0 + (tf32 ? 0 : 4) + li)) return st;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)grid, 1, 1);
   cfg.blockDim = dim3(kWThreads, 1, 1);
@@ -517,7 +495,7 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, gstate);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }

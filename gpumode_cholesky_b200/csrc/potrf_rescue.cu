@@ -1,12 +1,14 @@
-// FP32 rescue of the matrices the pivot guard flagged (guard.cuh).
+// Pivot audit and FP32 rescue of the pivot guard (guard.cuh).
 //
-// The guarded tensor-mode kernels (potrf_fused.cu, potrf_fused_ws.cu,
-// potrf_split.cu) record, per matrix, the first block column whose pivots
-// the mixed update could not resolve (guard state: int32 per matrix, -1 for
-// none).  Right after them, on the same stream, this kernel refactors every
-// flagged matrix from its first column in plain FP32 and overwrites its L
-// and info; unflagged matrices are not touched, and a launch with nothing
-// flagged returns at once (one scan of the guard state per CTA).
+// Right after a tensor-mode path (potrf_fused.cu, potrf_fused_ws.cu,
+// potrf_split.cu) has factored a batch, on the same stream, this kernel
+//   1. audits every matrix's computed pivots L_jj^2 against the mode's
+//      bound and writes the first failing block column per matrix, or -1,
+//      into the guard state (matrices dealt round-robin to the CTAs; one
+//      strided pass over the diagonals of A and L);
+//   2. after a grid barrier, returns when no matrix failed (the usual case);
+//   3. otherwise refactors every failing matrix from its first column in
+//      plain FP32 and overwrites its L and info; the others are not touched.
 //
 // Schedule: one cooperative launch, one CTA per SM (all CTAs resident at
 // once), left-looking by 64-wide block columns.  In column k the jobs are
@@ -71,8 +73,8 @@ __device__ __forceinline__ bool rescue_grid_sync(int* bar, int* s_ok) {
 }
 
 __global__ void __launch_bounds__(kRThreads, 1)
-    potrf_rescue_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                        const int32_t* __restrict__ gstate, int* bar, int32_t* __restrict__ info) {
+    potrf_rescue_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n, int mode,
+                        int32_t* __restrict__ gstate, int* bar, int32_t* __restrict__ info) {
   extern __shared__ unsigned char rraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(rraw) + 127) & ~(uintptr_t)127);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kRDiagOff);
@@ -84,7 +86,36 @@ __global__ void __launch_bounds__(kRThreads, 1)
   const int N = n / 64;
   const size_t n2 = (size_t)n * n;
 
-  // Fast exit: nothing flagged (the usual case).
+  // 1. Audit: the first block column whose pivot fails, per matrix.
+  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
+    const float* ad = a + (size_t)b * n2;
+    const float* ld = l + (size_t)b * n2;
+    int first = 0x7fffffff;
+    for (int j = 64 + tid; j < n; j += kRThreads) {
+      const float ljj = __ldcg(ld + (size_t)j * (n + 1));
+      const float ajj = __ldg(ad + (size_t)j * (n + 1));
+      if (!(ljj * ljj > guard_tau(mode, j >> 6) * ajj)) {
+        first = j >> 6;
+        break;
+      }
+    }
+    first = __reduce_min_sync(0xffffffffu, first);
+    if (lane == 0) misc[4 + warp] = first;
+    __syncthreads();
+    if (tid == 0) {
+      int m = misc[4];
+      for (int w = 1; w < kRThreads / 32; ++w) m = min(m, misc[4 + w]);
+      gstate[b] = m == 0x7fffffff ? -1 : m;
+    }
+    __syncthreads();
+  }
+  if (!rescue_grid_sync(bar, misc + 1)) {
+    if (tid == 0 && info != nullptr)
+      for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) info[b] = -1;
+    return;
+  }
+
+  // 2. Fast exit: nothing flagged (the usual case).
   bool any = false;
   for (int64_t b = tid; b < batch; b += kRThreads) any |= __ldcg(gstate + b) >= 0;
   if (!__syncthreads_or(any)) return;
@@ -180,7 +211,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
   }
 }
 
-int guard_rescue(const float* a, float* l, int64_t batch, int n, const int32_t* gstate, int* bar, int32_t* info,
+int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, int* bar, int32_t* info,
                  cudaStream_t s) {
   if (batch == 0) return B2P_OK;
   cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(int), s);
@@ -197,7 +228,7 @@ int guard_rescue(const float* a, float* l, int64_t batch, int n, const int32_t* 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   TraceScope ts(kKRescue, s);
-  e = cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, gstate, bar, info);
+  e = cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, mode, gstate, bar, info);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_rescue_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }

@@ -45,7 +45,6 @@
 #include <mutex>
 
 #include "diag64.cuh"
-#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -476,8 +475,7 @@ constexpr uint32_t kSZero = 81920;     // zeros for the strip's bulk stores
 constexpr uint32_t kSZeroBytes = 4096;
 constexpr uint32_t kSDiag = kSZero + kSZeroBytes;
 constexpr uint32_t kSBar = kSDiag + (((uint32_t)sizeof(Diag64Smem) + 127u) & ~127u);
-constexpr uint32_t kSADiag = kSBar + 64;  // A's diagonal of the current block (guard)
-constexpr uint32_t kSSmemBytes = kSADiag + 256 + 1024;
+constexpr uint32_t kSSmemBytes = kSBar + 64 + 1024;
 constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the CTA's rows
 
 // Column k of every matrix, G CTAs per matrix.  P = base - X_{k-1} X_{k-1,kk}^T
@@ -486,18 +484,11 @@ constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the
 // from its panel copy.  Then: factor the diagonal block (every CTA), solve
 // the CTA's 128-row chunks by forward substitution (one row per thread,
 // which is also one TMEM lane per thread), write L and the panel copy.
-//
-// With the pivot guard (GUARD; guard.cuh), the matrix's first CTA (g = 0)
-// sets gstate[b] = -1 in step 0; in later steps its warp 0 checks the
-// factored diagonal block, unless an earlier step has already recorded a
-// column for the matrix, and records k on a failure (A's diagonal is loaded
-// before the newest panel's product, so its latency is hidden).  The caller
-// runs the FP32 rescue (potrf_rescue.cu) after the last step.
-template <int MODE, bool GUARD>
+template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info, int32_t* __restrict__ gstate) {
+                      int32_t* __restrict__ info) {
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -505,7 +496,6 @@ __global__ void __launch_bounds__(kSThreads, 1)
   uint64_t* done = full + 1;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSBar + 16);
   int* flag = reinterpret_cast<int*>(sm + kSBar + 24);
-  float* adiag = reinterpret_cast<float*>(sm + kSADiag);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int N = n / 64, k0 = 64 * k;
   const int chunks = (n - k0 - 64 + kSThreads - 1) / kSThreads;
@@ -541,15 +531,6 @@ __global__ void __launch_bounds__(kSThreads, 1)
     uint8_t* W1 = W0 + rbytes;
     const float* base = (k >= 2) ? pbuf + (size_t)b * n * 64 : a + (size_t)b * n2 + k0;
     const size_t bld = (k >= 2) ? 64 : (size_t)n;
-    // Guard: this CTA checks the block unless the matrix has tripped already.
-    if (GUARD && !upd && g == 0 && tid == 0) gstate[b] = -1;
-    const bool gchk = GUARD && upd && g == 0 && gstate[b] < 0;
-    float ad0 = 0.f, ad1 = 0.f;
-    if (gchk && warp == 0) {
-      const float* ad = a + (size_t)b * n2 + (size_t)k0 * (n + 1);
-      ad0 = __ldg(ad + (size_t)(tid & 31) * (n + 1));
-      ad1 = __ldg(ad + (size_t)((tid & 31) + 32) * (n + 1));
-    }
 
     // The newest panel's product for the diagonal rows and chunk q (or the
     // diagonal rows only when q is out of range); false on a timeout.
@@ -616,17 +597,9 @@ __global__ void __launch_bounds__(kSThreads, 1)
         }
       }
     }
-    if (gchk && warp == 0) {
-      adiag[tid & 31] = ad0;
-      adiag[(tid & 31) + 32] = ad1;
-    }
     umma::fence_before_sync();
     __syncthreads();
     const int bad = diag64_factor(dg);
-    if (gchk && warp == 0 && bad != kDiagTimeout &&
-        guard_pivots_fail(dg.S, kD64Ld, adiag, guard_tau<MODE>(k), tid & 31)) {
-      if ((tid & 31) == 0) gstate[b] = k;
-    }
     if (g == 0) {
       for (int e = tid; e < 64 * 16; e += kSThreads) {
         const int r = e >> 4, c = (e & 15) * 4;
@@ -806,7 +779,7 @@ int side_stream(SideStream** out) {
 // wide kernel keeps to a bounded number of SMs so that the steps, which
 // carry the critical path, always find free ones.
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, int32_t* gstate) {
+                int32_t* info, cudaStream_t s) {
   const size_t need = split_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -817,16 +790,12 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   pb[0] = reinterpret_cast<float*>(copies + (size_t)batch * 2 * panel_copy_region_bytes(n));
   pb[1] = pb[0] + (size_t)batch * n * 64;
   const int64_t sms = device_sms();
-  const bool guard = (mode & B2P_FLAG_GUARD) && gstate != nullptr;
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
   auto upd = tf32 ? split_update_kernel<B2P_MODE_TF32> : split_update_kernel<B2P_MODE_BF16X3>;
-  auto stp = tf32 ? (guard ? split_step_kernel<B2P_MODE_TF32, true> : split_step_kernel<B2P_MODE_TF32, false>)
-                  : (guard ? split_step_kernel<B2P_MODE_BF16X3, true> : split_step_kernel<B2P_MODE_BF16X3, false>);
+  auto stp = tf32 ? split_step_kernel<B2P_MODE_TF32> : split_step_kernel<B2P_MODE_BF16X3>;
   auto wdk = tf32 ? split_wide_kernel<B2P_MODE_TF32> : split_wide_kernel<B2P_MODE_BF16X3>;
   if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, tf32 ? kSlotSplitU0 : kSlotSplitU1)) return st;
-  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes,
-                                guard ? (tf32 ? kSlotSplitSG0 : kSlotSplitSG1) : (tf32 ? kSlotSplitS0 : kSlotSplitS1)))
-    return st;
+  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, tf32 ? kSlotSplitS0 : kSlotSplitS1)) return st;
   const int N = n / 64;
   const int64_t n2 = (int64_t)n * n;
   const bool wide = n >= kWideMinN;
@@ -939,8 +908,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       const double rows = (double)(n - 64 * k - 64);
       TraceScope ts(kKSplitStep, s,
                     batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
-      const cudaError_t e =
-          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, gstate);
+      const cudaError_t e = cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,
