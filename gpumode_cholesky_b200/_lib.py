@@ -85,6 +85,7 @@ SIGNATURES = {
     "b2p_potrf_backward_workspace_size": (_c_sz, [_c_i64, _c_i64]),
     "b2p_potrf_backward": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, _c_i64, ctypes.c_int, _c_p, _c_sz, _c_p]),
     "b2p_debug_tc_gemm": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, ctypes.c_int, _c_p, _c_p]),
+    "b2p_debug_tc_gemm_stall": (ctypes.c_int, [_c_p, _c_p, _c_p, _c_i64, ctypes.c_int, ctypes.c_uint32, _c_p, _c_p]),
     "b2p_trace_enable": (ctypes.c_int, [ctypes.c_int]),
     "b2p_trace_read": (ctypes.c_int, [_c_p, _c_p, ctypes.c_int]),
     "b2p_trace_read_units": (ctypes.c_int, [_c_p, ctypes.c_int]),

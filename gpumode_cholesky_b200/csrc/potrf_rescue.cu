@@ -86,28 +86,33 @@ __global__ void __launch_bounds__(kRThreads, 1)
   const int N = n / 64;
   const size_t n2 = (size_t)n * n;
 
-  // 1. Audit: the first block column whose pivot fails, per matrix.
-  for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) {
-    const float* ad = a + (size_t)b * n2;
-    const float* ld = l + (size_t)b * n2;
-    int first = 0x7fffffff;
-    for (int j = 64 + tid; j < n; j += kRThreads) {
-      const float ljj = __ldcg(ld + (size_t)j * (n + 1));
-      const float ajj = __ldg(ad + (size_t)j * (n + 1));
-      if (!(ljj * ljj > guard_tau(mode, j >> 6) * ajj)) {
-        first = j >> 6;
-        break;
+  // 1. Audit: the first block column whose pivot fails, per matrix.  Each
+  //    CTA takes a contiguous range of matrices, its threads stride over all
+  //    their (matrix, pivot) pairs at once, and the first failing column of
+  //    each matrix is an atomic minimum in shared memory (the list area,
+  //    kRList * 2 ints, in rounds when the range is longer).
+  {
+    int* first = reinterpret_cast<int*>(list);
+    const int64_t per = (batch + gridDim.x - 1) / gridDim.x;
+    const int64_t lo0 = per * (int64_t)blockIdx.x;
+    const int64_t lo = lo0 < batch ? lo0 : batch, hi = lo + per < batch ? lo + per : batch;
+    const int npiv = n - 64;  // pivots 64 .. n-1 (block column 0 has no update)
+    for (int64_t r0 = lo; r0 < hi; r0 += 2 * kRList) {
+      const int cnt = (int)(hi - r0 < 2 * kRList ? hi - r0 : 2 * kRList);
+      for (int i = tid; i < cnt; i += kRThreads) first[i] = 0x7fffffff;
+      __syncthreads();
+      const int64_t total = (int64_t)cnt * npiv;
+#pragma unroll 4
+      for (int64_t e = tid; e < total; e += kRThreads) {
+        const int i = (int)(e / npiv), j = 64 + (int)(e - (int64_t)i * npiv);
+        const size_t off = (size_t)(r0 + i) * n2 + (size_t)j * (n + 1);
+        const float ljj = __ldcg(l + off), ajj = __ldg(a + off);
+        if (!(ljj * ljj > guard_tau(mode, j >> 6) * ajj)) atomicMin(first + i, j >> 6);
       }
+      __syncthreads();
+      for (int i = tid; i < cnt; i += kRThreads) gstate[r0 + i] = first[i] == 0x7fffffff ? -1 : first[i];
+      __syncthreads();
     }
-    first = __reduce_min_sync(0xffffffffu, first);
-    if (lane == 0) misc[4 + warp] = first;
-    __syncthreads();
-    if (tid == 0) {
-      int m = misc[4];
-      for (int w = 1; w < kRThreads / 32; ++w) m = min(m, misc[4 + w]);
-      gstate[b] = m == 0x7fffffff ? -1 : m;
-    }
-    __syncthreads();
   }
   if (!rescue_grid_sync(bar, misc + 1)) {
     if (tid == 0 && info != nullptr)

@@ -114,6 +114,7 @@ struct TcShared {
   uint64_t* mbar;
   uint32_t* tslot;
   int* flag;
+  uint64_t* stall;  // an mbarrier nothing arrives on (the diagnostic's timed-out wait)
 };
 
 __device__ __forceinline__ TcShared tc_layout(unsigned char* raw) {
@@ -124,6 +125,7 @@ __device__ __forceinline__ TcShared tc_layout(unsigned char* raw) {
   s.mbar = reinterpret_cast<uint64_t*>(base + 2 * kTcOperandBytes);
   s.tslot = reinterpret_cast<uint32_t*>(base + 2 * kTcOperandBytes + 8);
   s.flag = reinterpret_cast<int*>(base + 2 * kTcOperandBytes + 16);
+  s.stall = reinterpret_cast<uint64_t*>(base + 2 * kTcOperandBytes + 24);
   return s;
 }
 
@@ -135,6 +137,7 @@ __device__ __forceinline__ void tc_setup(const TcShared& sh) {
   }
   if (threadIdx.x == 32) {
     umma::mbar_init(sh.mbar, 1);
+    umma::mbar_init(sh.stall, 1);
     umma::mbar_fence_init();
   }
   umma::fence_before_sync();
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_gemm_test_kernel(const float* __restrict__ a, const float* __restrict__ bmat, float* __restrict__ d,
-                        int64_t count, int32_t* __restrict__ err) {
+                        int64_t count, int32_t* __restrict__ err, uint32_t stall_polls) {
   extern __shared__ unsigned char tc_raw[];
   const TcShared sh = tc_layout(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -294,6 +297,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     umma::fence_before_sync();
     __syncthreads();
+    if (stall_polls != 0) {
+      // Diagnostic: a bounded wait on a barrier nothing completes runs out
+      // and takes the same error path as a real timeout.  The tile's MMAs
+      // have completed, so nothing is in flight and no drain is needed.
+      const bool got = umma::mbar_wait_bounded(sh.stall, 0u, stall_polls);
+      if (!got) *sh.flag = 1;
+      __syncthreads();
+      if (*sh.flag) {
+        if (tid == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
+        tc_teardown(sh, tmem, true, parity);
+        return;
+      }
+    }
   }
   if (!ok && tid == 0 && err != nullptr) atomicExch(err, B2P_ERR_TIMEOUT);
   tc_teardown(sh, tmem, ok, parity);
@@ -350,6 +366,11 @@ using namespace b2p;
 
 extern "C" int b2p_debug_tc_gemm(const float* a, const float* bmat, float* d, int64_t count, int mode,
                                  int32_t* err, void* stream) {
+  return b2p_debug_tc_gemm_stall(a, bmat, d, count, mode, 0u, err, stream);
+}
+
+extern "C" int b2p_debug_tc_gemm_stall(const float* a, const float* bmat, float* d, int64_t count, int mode,
+                                       uint32_t stall_polls, int32_t* err, void* stream) {
   if (count < 0 || a == nullptr || bmat == nullptr || d == nullptr)
     return set_error(B2P_ERR_INVALID_ARG, "bad arguments to b2p_debug_tc_gemm");
   if (count == 0) return B2P_OK;
@@ -358,10 +379,11 @@ extern "C" int b2p_debug_tc_gemm(const float* a, const float* bmat, float* d, in
   const int m = mode & B2P_MODE_MASK;
   if (m == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)tc_gemm_test_kernel<B2P_MODE_TF32>, kTcSmemBytes, kSlotTc2)) return st;
-    tc_gemm_test_kernel<B2P_MODE_TF32><<<grid, kTcThreads, kTcSmemBytes, s>>>(a, bmat, d, count, err);
+    tc_gemm_test_kernel<B2P_MODE_TF32><<<grid, kTcThreads, kTcSmemBytes, s>>>(a, bmat, d, count, err, stall_polls);
   } else if (m == B2P_MODE_BF16X3) {
     if (int st = ensure_smem_attr((const void*)tc_gemm_test_kernel<B2P_MODE_BF16X3>, kTcSmemBytes, kSlotTc3)) return st;
-    tc_gemm_test_kernel<B2P_MODE_BF16X3><<<grid, kTcThreads, kTcSmemBytes, s>>>(a, bmat, d, count, err);
+    tc_gemm_test_kernel<B2P_MODE_BF16X3><<<grid, kTcThreads, kTcSmemBytes, s>>>(a, bmat, d, count, err,
+                                                                                  stall_polls);
   } else {
     return set_error(B2P_ERR_UNSUPPORTED, "b2p_debug_tc_gemm supports tf32 and bf16x3");
   }

@@ -316,6 +316,19 @@ B2P_API int b2p_debug_tc_gemm(const float* a, const float* b, float* d, int64_t 
                               int32_t* err, void* stream);
 
 /*
+ * Diagnostic of the bounded-wait error path: b2p_debug_tc_gemm, where every
+ * CTA, after its first pair's product is written, waits `stall_polls` polls
+ * on an mbarrier that nothing arrives on.  The wait runs out, the kernel
+ * writes B2P_ERR_TIMEOUT to err, releases its tensor memory and returns, and
+ * the context stays usable (the pairs after each CTA's first are not
+ * computed).  The same path ends every other bounded wait of the library;
+ * this makes it testable without a fault.  stall_polls = 0 is
+ * b2p_debug_tc_gemm.  No counterpart in the reference.
+ */
+B2P_API int b2p_debug_tc_gemm_stall(const float* a, const float* b, float* d, int64_t count, int mode,
+                                    uint32_t stall_polls, int32_t* err, void* stream);
+
+/*
  * Launch trace: when enabled, every kernel the library launches is bracketed
  * by a pair of CUDA events recorded on its launch stream, so a caller can
  * read per-kernel device time (the counterpart of the reference's in-kernel
