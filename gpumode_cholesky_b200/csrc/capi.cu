@@ -115,7 +115,7 @@ int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int pat
 // Whether a call on `path` runs the pivot guard (and so its rescue).
 static bool guarded(int path, int mode) {
   const int m = mode & B2P_MODE_MASK;
-  return (mode & B2P_FLAG_GUARD) && (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3) &&
+  return (mode & B2P_FLAG_GUARD) && (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3 || m == B2P_MODE_FP8) &&
          (path == B2P_PATH_FUSED || path == B2P_PATH_FUSED_WS || path == B2P_PATH_SPLIT);
 }
 

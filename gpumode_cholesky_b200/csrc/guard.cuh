@@ -5,6 +5,7 @@
 // entry of D carries an error of about
 //     delta(k) * sum_c L_jc^2  <=  delta(k) * A_jj,
 //     delta(k) = 2^-16 (BF16x3: the operand split hi + lo keeps 16 bits)
+//              | 2^-12 (FP8: E4M3 cross terms, panel_copy.cuh)
 //              | 2^-10 (TF32: 11-bit operands, product error 2^-10)
 //                + (MMAs accumulated so far) * 2^-23 (the accumulator does
 //                  not round to nearest: one FP32 ulp per accumulation step),
@@ -49,9 +50,10 @@ constexpr int kGuardStageFloats = 64 * kGuardStageLd;
 // 0 for column 0, which no update precedes.
 __device__ __forceinline__ float guard_tau(int mode, int k) {
   if (k == 0) return 0.0f;
-  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  const float rep = tf32 ? 9.765625e-4f : 1.52587890625e-5f;  // 2^-10, 2^-16
-  const float steps = tf32 ? 8.0f : 12.0f;                     // MMAs per 64-wide chunk
+  const int m = mode & B2P_MODE_MASK;
+  // Operand rounding: 2^-10 (TF32), 2^-12 (FP8: E4M3 cross terms), 2^-16 (BF16x3).
+  const float rep = m == B2P_MODE_TF32 ? 9.765625e-4f : m == B2P_MODE_FP8 ? 2.44140625e-4f : 1.52587890625e-5f;
+  const float steps = m == B2P_MODE_BF16X3 ? 12.0f : 8.0f;  // MMAs per 64-wide chunk
   return kGuardMargin * (rep + steps * (float)k * 1.1920928955078125e-7f);  // 2^-23 per step
 }
 

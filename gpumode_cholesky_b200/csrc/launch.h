@@ -200,6 +200,9 @@ enum SmemSlot {
   kSlotTrsv1,
   kSlotGpForward,
   kSlotRescue,
+  kSlotSplitU2,
+  kSlotSplitS2,
+  kSlotSplitW2,
   kSlotCount
 };
 

@@ -72,7 +72,8 @@ static_assert(128 * kUParkLd * 4 <= kUStaging, "parked accumulator must fit the 
 template <int MODE>
 __global__ void __launch_bounds__(kUThreads, 2)
     split_update_kernel(const float* base, int64_t base_mstride, int base_ld, const uint8_t* __restrict__ ws,
-                        float* pout, int n, int k, int c_begin, int c_end, int segs, int32_t* __restrict__ info) {
+                        float* pout, int n, int k, int c_begin, int c_end, int segs, int32_t* __restrict__ info,
+                        const float* __restrict__ sig) {
   extern __shared__ unsigned char uraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(uraw) + 1023) & ~(uintptr_t)1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kUStaging);  // [2]
@@ -173,8 +174,11 @@ __global__ void __launch_bounds__(kUThreads, 2)
   __syncthreads();
   const bool ok = *flag == 0;
   if (ok) {
-    // Park U_s: thread -> accumulator row (TMEM lane) 32w + lane.
+    // Park U_s: thread -> accumulator row (TMEM lane) 32w + lane.  FP8: the
+    // accumulator holds 256 U / (s_row s_k) (panel_copy.cuh).
     const int rl = 32 * warp + lane;
+    float sc = 1.0f;
+    if (MODE == B2P_MODE_FP8) sc = sig[(size_t)b * N + min(r0 + rl, n - 1) / 64] * sig[(size_t)b * N + k] * kFp8Fold;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       float d[32];
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
 #pragma unroll
       for (int q = 0; q < 8; ++q)
         *reinterpret_cast<float4*>(park + rl * kUParkLd + 32 * h + 4 * q) =
-            make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+            make_float4(d[4 * q] * sc, d[4 * q + 1] * sc, d[4 * q + 2] * sc, d[4 * q + 3] * sc);
     }
   } else if (tid == 0 && info != nullptr) {
     info[b] = -1;
@@ -251,7 +255,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kXThreads, 1)
     split_wide_kernel(const float* base, int64_t base_mstride, int base_ld, const uint8_t* __restrict__ ws,
                       float* out, int64_t out_mstride, int out_ld, int64_t batch, int n, int j0, int nbw,
-                      int c_begin, int c_end, int segs, int32_t* __restrict__ info) {
+                      int c_begin, int c_end, int segs, int32_t* __restrict__ info, const float* __restrict__ sig) {
   extern __shared__ unsigned char xraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(xraw) + 1023) & ~(uintptr_t)1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(sm + kXStaging);  // [2] stage loaded
@@ -379,6 +383,13 @@ __global__ void __launch_bounds__(kXThreads, 1)
       float acc[128];
 #pragma unroll
       for (int c = 0; c < 128; ++c) acc[c] = 0.0f;
+      // FP8: the accumulators hold 256 U / (s_row s_col) per 64-column block.
+      float sc[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+      if (MODE == B2P_MODE_FP8) {
+        const float sr = sig[(size_t)b * N + min(r0 + rl, n - 1) / 64] * kFp8Fold;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sc[j] = sr * sig[(size_t)b * N + min(j0 + cj + 128 * hh + 32 * j, n - 1) / 64];
+      }
       bool ok = true;
       for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int p = (int)(gc & 1);
@@ -393,7 +404,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
           float d[32];
           umma::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(p * kXCols + 128 * hh + 32 * j), d);
 #pragma unroll
-          for (int c = 0; c < 32; ++c) acc[32 * j + c] += d[c];
+          for (int c = 0; c < 32; ++c) acc[32 * j + c] = fmaf(d[c], sc[j], acc[32 * j + c]);
         }
         umma::fence_before_sync();
         __syncwarp();
@@ -488,7 +499,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 1)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info) {
+                      int32_t* __restrict__ info, const float* __restrict__ sig) {
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -580,6 +591,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
     if (warp < 2) {
       const float4* src = reinterpret_cast<const float4*>(base + (size_t)(k0 + tid) * bld);
       float4* dst = reinterpret_cast<float4*>(dg.S + tid * kD64Ld);
+      // FP8: the accumulator holds 256 D / s_k^2 (panel_copy.cuh).
+      const float sd = MODE == B2P_MODE_FP8 ? sig[(size_t)b * N + k] * sig[(size_t)b * N + k] * kFp8Fold : 1.0f;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         float d[32];
@@ -592,8 +605,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
 #pragma unroll
         for (int c4 = 0; c4 < 8; ++c4) {
           const float4 v = src[8 * h + c4];
-          dst[8 * h + c4] =
-              make_float4(v.x - d[4 * c4], v.y - d[4 * c4 + 1], v.z - d[4 * c4 + 2], v.w - d[4 * c4 + 3]);
+          dst[8 * h + c4] = make_float4(v.x - d[4 * c4] * sd, v.y - d[4 * c4 + 1] * sd, v.z - d[4 * c4 + 2] * sd,
+                                        v.w - d[4 * c4 + 3] * sd);
         }
       }
     }
@@ -649,29 +662,33 @@ __global__ void __launch_bounds__(kSThreads, 1)
       if (r < n) {
         float x[64];
         const float4* src = reinterpret_cast<const float4*>(base + (size_t)r * bld);
+        // FP8: the accumulator holds 256 D / (s_r s_k).
+        const float sr =
+            MODE == B2P_MODE_FP8 ? sig[(size_t)b * N + r / 64] * sig[(size_t)b * N + k] * kFp8Fold : 1.0f;
 #pragma unroll
         for (int c4 = 0; c4 < 8; ++c4) {
           const float4 v = src[c4];
-          x[4 * c4 + 0] = v.x - d0[4 * c4 + 0];
-          x[4 * c4 + 1] = v.y - d0[4 * c4 + 1];
-          x[4 * c4 + 2] = v.z - d0[4 * c4 + 2];
-          x[4 * c4 + 3] = v.w - d0[4 * c4 + 3];
+          x[4 * c4 + 0] = v.x - d0[4 * c4 + 0] * sr;
+          x[4 * c4 + 1] = v.y - d0[4 * c4 + 1] * sr;
+          x[4 * c4 + 2] = v.z - d0[4 * c4 + 2] * sr;
+          x[4 * c4 + 3] = v.w - d0[4 * c4 + 3] * sr;
           const float4 w = src[8 + c4];
-          x[32 + 4 * c4 + 0] = w.x - d1[4 * c4 + 0];
-          x[32 + 4 * c4 + 1] = w.y - d1[4 * c4 + 1];
-          x[32 + 4 * c4 + 2] = w.z - d1[4 * c4 + 2];
-          x[32 + 4 * c4 + 3] = w.w - d1[4 * c4 + 3];
+          x[32 + 4 * c4 + 0] = w.x - d1[4 * c4 + 0] * sr;
+          x[32 + 4 * c4 + 1] = w.y - d1[4 * c4 + 1] * sr;
+          x[32 + 4 * c4 + 2] = w.z - d1[4 * c4 + 2] * sr;
+          x[32 + 4 * c4 + 3] = w.w - d1[4 * c4 + 3] * sr;
         }
         panel_solve64(x, dg);
         float4* dst = reinterpret_cast<float4*>(L + (size_t)r * n + k0);
 #pragma unroll
         for (int c4 = 0; c4 < 16; ++c4) dst[c4] = make_float4(x[4 * c4], x[4 * c4 + 1], x[4 * c4 + 2], x[4 * c4 + 3]);
         if (k + 1 < N) {
+          const float isig = MODE == B2P_MODE_FP8 ? 1.0f / sig[(size_t)b * N + r / 64] : 1.0f;
 #pragma unroll
           for (int c8 = 0; c8 < 8; ++c8) {
             const float v[8] = {x[8 * c8],     x[8 * c8 + 1], x[8 * c8 + 2], x[8 * c8 + 3],
                                 x[8 * c8 + 4], x[8 * c8 + 5], x[8 * c8 + 6], x[8 * c8 + 7]};
-            panel_copy_store<MODE>(W0, W1, N, k, r, c8, v);
+            panel_copy_store<MODE>(W0, W1, N, k, r, c8, v, isig);
           }
         }
       }
@@ -694,8 +711,24 @@ __global__ void __launch_bounds__(kSThreads, 1)
 
 bool split_supported(int64_t n, int mode) {
   const int m = mode & B2P_MODE_MASK;
-  return (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3) && !(mode & B2P_FLAG_FP64_DIAG) && n > 128 &&
-         (n % 64) == 0 && n <= 65536;
+  return (m == B2P_MODE_TF32 || m == B2P_MODE_BF16X3 || m == B2P_MODE_FP8) && !(mode & B2P_FLAG_FP64_DIAG) &&
+         n > 128 && (n % 64) == 0 && n <= 65536;
+}
+
+// FP8 mode: the power-of-two scale of every 64-row block of every matrix,
+// s = 2^ceil(log2(max_{rows i of the block} sqrt(A_ii) / 256)), so that
+// |L[i][j]| <= sqrt(A_ii) <= 256 s (panel_copy.cuh).  One thread per block.
+__global__ void fp8_scale_kernel(const float* __restrict__ a, float* __restrict__ sig, int64_t batch, int n) {
+  const int N = n / 64;
+  const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= batch * N) return;
+  const int64_t b = id / N;
+  const int blk = (int)(id - b * N);
+  const float* d = a + (size_t)b * n * n + (size_t)(64 * blk) * (n + 1);
+  float m = 0.0f;
+  for (int i = 0; i < 64; ++i) m = fmaxf(m, __ldg(d + (size_t)i * (n + 1)));
+  const float v = sqrtf(m) * (1.0f / 256.0f);
+  sig[id] = (v > 0.0f && isfinite(v)) ? exp2f(ceilf(log2f(v))) : 1.0f;
 }
 
 // Orders from which the older panels are applied an outer block at a time
@@ -708,10 +741,14 @@ static_assert(64 * kWideCols % kXCols == 0, "outer blocks are whole wide tiles")
 // Panel copies, then two per-matrix FP32 panel buffers (n x 64 each; block
 // columns alternate between them), then for large orders two per-matrix
 // outer-block buffers (n x 512 each, alternating by outer block).
-size_t split_workspace_bytes(int64_t batch, int64_t n) {
+static size_t split_sig_offset(int64_t batch, int64_t n) {
   size_t bytes = (size_t)batch * 2 * panel_copy_region_bytes((int)n) + 2 * (size_t)batch * n * 64 * sizeof(float);
   if (n >= kWideMinN) bytes += 2 * (size_t)batch * n * 64 * kWideCols * sizeof(float);
-  return bytes + 1024;
+  return bytes;
+}
+size_t split_workspace_bytes(int64_t batch, int64_t n) {
+  // ... then the FP8 mode's block scales (batch x n/64 floats).
+  return split_sig_offset(batch, n) + (((size_t)batch * (n / 64) * sizeof(float) + 255) & ~(size_t)255) + 1024;
 }
 
 namespace {
@@ -790,12 +827,25 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   pb[0] = reinterpret_cast<float*>(copies + (size_t)batch * 2 * panel_copy_region_bytes(n));
   pb[1] = pb[0] + (size_t)batch * n * 64;
   const int64_t sms = device_sms();
-  const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  auto upd = tf32 ? split_update_kernel<B2P_MODE_TF32> : split_update_kernel<B2P_MODE_BF16X3>;
-  auto stp = tf32 ? split_step_kernel<B2P_MODE_TF32> : split_step_kernel<B2P_MODE_BF16X3>;
-  auto wdk = tf32 ? split_wide_kernel<B2P_MODE_TF32> : split_wide_kernel<B2P_MODE_BF16X3>;
-  if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, tf32 ? kSlotSplitU0 : kSlotSplitU1)) return st;
-  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, tf32 ? kSlotSplitS0 : kSlotSplitS1)) return st;
+  const int m = mode & B2P_MODE_MASK;
+  const int mi = m == B2P_MODE_TF32 ? 0 : m == B2P_MODE_BF16X3 ? 1 : 2;
+  auto upd = mi == 0 ? split_update_kernel<B2P_MODE_TF32>
+             : mi == 1 ? split_update_kernel<B2P_MODE_BF16X3> : split_update_kernel<B2P_MODE_FP8>;
+  auto stp = mi == 0 ? split_step_kernel<B2P_MODE_TF32>
+             : mi == 1 ? split_step_kernel<B2P_MODE_BF16X3> : split_step_kernel<B2P_MODE_FP8>;
+  auto wdk = mi == 0 ? split_wide_kernel<B2P_MODE_TF32>
+             : mi == 1 ? split_wide_kernel<B2P_MODE_BF16X3> : split_wide_kernel<B2P_MODE_FP8>;
+  const int uslot[3] = {kSlotSplitU0, kSlotSplitU1, kSlotSplitU2};
+  const int sslot[3] = {kSlotSplitS0, kSlotSplitS1, kSlotSplitS2};
+  const int wslot[3] = {kSlotSplitW0, kSlotSplitW1, kSlotSplitW2};
+  if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, uslot[mi])) return st;
+  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, sslot[mi])) return st;
+  float* sig = reinterpret_cast<float*>(copies + split_sig_offset(batch, n));
+  if (m == B2P_MODE_FP8) {
+    const int64_t blocks = batch * (n / 64);
+    fp8_scale_kernel<<<(unsigned)((blocks + 127) / 128), 128, 0, s>>>(a, sig, batch, n);
+    if (int st = check_launch("fp8_scale_kernel")) return st;
+  }
   const int N = n / 64;
   const int64_t n2 = (int64_t)n * n;
   const bool wide = n >= kWideMinN;
@@ -803,7 +853,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const int nbw = 64 * W;
   float* bw[2] = {nullptr, nullptr};
   if (wide) {
-    if (int st = ensure_smem_attr((const void*)wdk, kXSmemBytes, tf32 ? kSlotSplitW0 : kSlotSplitW1)) return st;
+    if (int st = ensure_smem_attr((const void*)wdk, kXSmemBytes, wslot[mi])) return st;
     bw[0] = pb[1] + (size_t)batch * n * 64;
     bw[1] = bw[0] + (size_t)batch * n * nbw;
   }
@@ -836,7 +886,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     cfg.numAttrs = 1;
     TraceScope ts(kKSplitUpdate, st, 2.0 * 64 * 64 * (double)(c1 - c0) * batch * (n - 64 * k));
     const cudaError_t e = cudaLaunchKernelEx(&cfg, upd, base, mstride, ld, (const uint8_t*)copies, pout, n, k,
-                                             c0, c1, segs, info);
+                                             c0, c1, segs, info, (const float*)sig);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_update_kernel: %s", cudaGetErrorString(e));
     return B2P_OK;
   };
@@ -866,7 +916,8 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     cfg.numAttrs = 1;
     TraceScope ts(kKSplitWide, side->wide, 2.0 * 64 * (double)c1 * cols * batch * (n - j0));
     const cudaError_t e = cudaLaunchKernelEx(&cfg, wdk, (const float*)(a + j0), n2, n, (const uint8_t*)copies,
-                                             bw[J & 1], (int64_t)n * nbw, nbw, batch, n, j0, cols, 0, c1, segs, info);
+                                             bw[J & 1], (int64_t)n * nbw, nbw, batch, n, j0, cols, 0, c1, segs, info,
+                                             (const float*)sig);
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_wide_kernel: %s", cudaGetErrorString(e));
     return B2P_OK;
   };
@@ -908,7 +959,8 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       const double rows = (double)(n - 64 * k - 64);
       TraceScope ts(kKSplitStep, s,
                     batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
-      const cudaError_t e = cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info);
+      const cudaError_t e =
+          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, (const float*)sig);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,

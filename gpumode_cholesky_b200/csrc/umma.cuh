@@ -31,7 +31,8 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t saddr) {
 }
 
 // Instruction descriptor: FP32 accumulate, K-major A and B, M x N tile.
-// fmt: 1 = BF16 operands (kind::f16), 2 = TF32 operands (kind::tf32).
+// fmt: 1 = BF16 operands (kind::f16), 2 = TF32 operands (kind::tf32),
+// 0 = E4M3 operands (kind::f8f6f4).
 __host__ __device__ constexpr uint32_t idesc_f32acc(int fmt, int m, int n) {
   return (1u << 4)                       // D format F32
          | ((uint32_t)fmt << 7)          // A format
@@ -82,6 +83,18 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint6
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+// D += A * B^T with E4M3 operands (K = 32 per instruction, 32 bytes of each
+// operand row), FP32 accumulation.
+__device__ __forceinline__ void mma_f8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
       : "memory");
 }
