@@ -101,13 +101,29 @@ __global__ void __launch_bounds__(kRThreads, 1)
       const int cnt = (int)(hi - r0 < 2 * kRList ? hi - r0 : 2 * kRList);
       for (int i = tid; i < cnt; i += kRThreads) first[i] = 0x7fffffff;
       __syncthreads();
-      const int64_t total = (int64_t)cnt * npiv;
-#pragma unroll 4
-      for (int64_t e = tid; e < total; e += kRThreads) {
-        const int i = (int)(e / npiv), j = 64 + (int)(e - (int64_t)i * npiv);
-        const size_t off = (size_t)(r0 + i) * n2 + (size_t)j * (n + 1);
-        const float ljj = __ldcg(l + off), ajj = __ldg(a + off);
-        if (!(ljj * ljj > guard_tau(mode, j >> 6) * ajj)) atomicMin(first + i, j >> 6);
+      // cnt <= 2 kRList and npiv < 2^16: the pair index fits 32 bits.  Eight
+      // pairs per thread are loaded before any is tested (latency-bound
+      // strided loads: one 32-byte sector each).
+      const int total = cnt * npiv;
+      for (int e0 = tid; e0 < total; e0 += 8 * kRThreads) {
+        float lv[8], av[8];
+        int iv[8], jv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int e = e0 + u * kRThreads;
+          iv[u] = e / npiv;
+          jv[u] = 64 + (e - iv[u] * npiv);
+          lv[u] = 1.0f;
+          av[u] = 0.0f;
+          if (e < total) {
+            const size_t off = (size_t)(r0 + iv[u]) * n2 + (size_t)jv[u] * (n + 1);
+            lv[u] = __ldcg(l + off);
+            av[u] = __ldg(a + off);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (!(lv[u] * lv[u] > guard_tau(mode, jv[u] >> 6) * av[u])) atomicMin(first + iv[u], jv[u] >> 6);
       }
       __syncthreads();
       for (int i = tid; i < cnt; i += kRThreads) gstate[r0 + i] = first[i] == 0x7fffffff ? -1 : first[i];
