@@ -1045,7 +1045,9 @@ def _roofline(workload: str, shapes, name: str, ms: float, count: int, units: fl
         flops = sum(_flops(b, n) for b, n in shapes)
     per_launch = flops / max(count, 1)
     achieved = flops / (ms / 1000.0) / 1e12
-    mode = modes[-1]
+    # The guard adds a separate launch and leaves the factorization kernels
+    # as they are, so their profiled traffic is that of the bare mode.
+    mode = modes[-1].split("+")[0]
     tpu = traffic_tab.get((name, workload, mode))
     return {
         "kernel": name,
