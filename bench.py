@@ -13,7 +13,8 @@ the plain FP32 form and cuSOLVER on the same GPU are reported beside it.
 
 Other workloads (profiling and extra lines, not the headline):
   small   4096 x 32 (HBM-bound; 8 rotating input sets, 256 MiB > L2)
-  large   1 x 8192 (GG^T/n + 0.1 I); large16k, large32k: 1 x 16384, 1 x 32768
+  large   1 x 8192 (GG^T/n + 0.1 I); large12k, large16k, large32k: 1 x 12288,
+          1 x 16384, 1 x 32768
   ragged  3000 matrices, n log-uniform in [16, 2048], packed (one ragged plan
           replayed from a CUDA graph; --autotune picks the plan options)
   gp      Gaussian-process loss, forward and backward through autograd
@@ -95,6 +96,14 @@ WORKLOADS = {
         "desc": "large potrf: 1x8192 FP32, GG^T/n+0.1I",
         "metric": "potrf us per step (1x8192)",
         "baseline_us": 5773.79,
+    },
+    "large12k": {
+        "shapes": [(1, 12288)],
+        "seeds": [412288],
+        "gen": "gram",
+        "sets": 1,
+        "desc": "large potrf: 1x12288 FP32, GG^T/n+0.1I (the first order with the outer-block update; profiling)",
+        "metric": "potrf us per step (1x12288)",
     },
     "large16k": {
         "shapes": [(1, 16384)],
