@@ -89,6 +89,7 @@ SIGNATURES = {
     "b2p_trace_enable": (ctypes.c_int, [ctypes.c_int]),
     "b2p_trace_read": (ctypes.c_int, [_c_p, _c_p, ctypes.c_int]),
     "b2p_trace_read_units": (ctypes.c_int, [_c_p, ctypes.c_int]),
+    "b2p_trace_read_starts": (ctypes.c_int, [_c_p, ctypes.c_int]),
     "b2p_kernel_name": (ctypes.c_char_p, [ctypes.c_int]),
 }
 
@@ -142,6 +143,7 @@ class LaunchTrace:
         self.capacity = capacity
         self._records: list[tuple[str, float]] = []
         self._units: list[float] = []
+        self._starts: list[float] = []
 
     def __enter__(self):
         check(load().b2p_trace_enable(self.capacity), "b2p_trace_enable")
@@ -156,11 +158,18 @@ class LaunchTrace:
         units = (ctypes.c_double * self.capacity)()
         ku = lib.b2p_trace_read_units(units, self.capacity)
         self._units = [float(units[i]) for i in range(min(k, ku))]
+        starts = (ctypes.c_float * self.capacity)()
+        ks = lib.b2p_trace_read_starts(starts, self.capacity)
+        self._starts = [float(starts[i]) for i in range(min(k, ks))]
         lib.b2p_trace_enable(0)
         return False
 
     def records(self) -> list[tuple[str, float]]:
         return list(self._records)
+
+    def timeline(self) -> list[tuple[str, float, float]]:
+        """(kernel name, start ms after the first launch, duration ms) per launch."""
+        return [(name, s, t) for (name, t), s in zip(self._records, self._starts)]
 
     def units(self) -> dict[str, float]:
         """Algorithmic work per kernel name, summed over its launches."""

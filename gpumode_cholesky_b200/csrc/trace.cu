@@ -87,6 +87,19 @@ int b2p_trace_read(int32_t* kernel_ids, float* ms, int max_entries) {
   return k;
 }
 
+int b2p_trace_read_starts(float* start_ms, int max_entries) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  int k = 0;
+  for (auto& e : g_entries) {
+    if (k >= max_entries) break;
+    float t = -1.0f;
+    if (cudaEventSynchronize(e.start) == cudaSuccess) cudaEventElapsedTime(&t, g_entries[0].start, e.start);
+    if (start_ms) start_ms[k] = t;
+    ++k;
+  }
+  return k;
+}
+
 int b2p_trace_read_units(double* units, int max_entries) {
   std::lock_guard<std::mutex> lock(g_mu);
   int k = 0;

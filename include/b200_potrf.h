@@ -337,6 +337,9 @@ B2P_API int b2p_debug_tc_gemm_stall(const float* a, const float* b, float* d, in
  *                               (0 stops recording and frees the events);
  *   b2p_trace_read(ids, ms, max) synchronises the recorded events and writes
  *                               kernel ids and durations; returns the count;
+ *   b2p_trace_read_starts(t, max) each recorded launch's start, in ms after
+ *                               the first recorded launch's (the launches'
+ *                               own streams: a timeline of concurrent work);
  *   b2p_trace_read_units(u, max) the algorithmic work of each recorded
  *                               launch, in the same order: n^3/3 flops per
  *                               matrix for kernels that factor whole
@@ -347,6 +350,7 @@ B2P_API int b2p_debug_tc_gemm_stall(const float* a, const float* b, float* d, in
  */
 B2P_API int b2p_trace_enable(int capacity);
 B2P_API int b2p_trace_read(int32_t* kernel_ids, float* ms, int max_entries);
+B2P_API int b2p_trace_read_starts(float* start_ms, int max_entries);
 B2P_API int b2p_trace_read_units(double* units, int max_entries);
 B2P_API const char* b2p_kernel_name(int id);
 
