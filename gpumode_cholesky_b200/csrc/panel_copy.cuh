@@ -103,11 +103,15 @@ __device__ __forceinline__ void panel_copy_store(uint8_t* w0, uint8_t* w1, int N
 }
 
 // D (128 x NB FP32 in TMEM) (+)= A B^T over one 64-wide column, from staged
-// copies: A = 128 rows at sa (region 0 at +0, region 1 at +16384), B = NB
-// rows at sb (region 0 at +0, region 1 at +128 NB).  One thread issues.
-template <int MODE, int NB = 64>
+// copies: A = 128 rows at sa (region 0 at +0, region 1 at +A1), B = NB rows
+// at sb (region 0 at +0, region 1 at +128 NB).  One thread issues.  A1 below
+// 16384 lets A overlap B's staging when only A's first A1 / 128 rows matter
+// (their accumulator lanes); the rows beyond read whatever follows in
+// shared memory.
+template <int MODE, int NB = 64, uint32_t A1 = 16384u>
 __device__ __forceinline__ void panel_copy_mmas(uint32_t d, uint32_t sa, uint32_t sb, bool acc) {
   static_assert(NB % 16 == 0 && NB >= 16 && NB <= 256, "MMA N for M = 128");
+  static_assert(A1 % 1024 == 0, "SW128 operands start on 1024-byte boundaries");
   constexpr uint32_t kB1 = 128u * NB;
   if (MODE == B2P_MODE_FP8) {
     // h h^T on kind::f16 (K = 16 per instruction), then q p^T and p q^T on
@@ -123,14 +127,14 @@ __device__ __forceinline__ void panel_copy_mmas(uint32_t d, uint32_t sa, uint32_
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const uint32_t o = (uint32_t)(s * 32);
-      umma::mma_f8(d, umma::desc_k_sw128(sa + 16384 + o), umma::desc_k_sw128(sb + kB1 + 64 + o), i8, 1u);
-      umma::mma_f8(d, umma::desc_k_sw128(sa + 16384 + 64 + o), umma::desc_k_sw128(sb + kB1 + o), i8, 1u);
+      umma::mma_f8(d, umma::desc_k_sw128(sa + A1 + o), umma::desc_k_sw128(sb + kB1 + 64 + o), i8, 1u);
+      umma::mma_f8(d, umma::desc_k_sw128(sa + A1 + 64 + o), umma::desc_k_sw128(sb + kB1 + o), i8, 1u);
     }
   } else if (MODE == B2P_MODE_TF32) {
     constexpr uint32_t idesc = umma::idesc_f32acc(2, 128, NB);
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-      const uint32_t ka = (uint32_t)((s >> 2) * 16384 + (s & 3) * 32);
+      const uint32_t ka = (uint32_t)((s >> 2) * A1 + (s & 3) * 32);
       const uint32_t kb = (uint32_t)((s >> 2) * kB1 + (s & 3) * 32);
       umma::mma_tf32(d, umma::desc_k_sw128(sa + ka), umma::desc_k_sw128(sb + kb), idesc, (acc || s > 0) ? 1u : 0u);
     }
@@ -139,7 +143,7 @@ __device__ __forceinline__ void panel_copy_mmas(uint32_t d, uint32_t sa, uint32_
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       const uint32_t o = (uint32_t)(s * 32);
-      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + 16384 + o);
+      const uint64_t ah = umma::desc_k_sw128(sa + o), al = umma::desc_k_sw128(sa + A1 + o);
       const uint64_t bh = umma::desc_k_sw128(sb + o), bl = umma::desc_k_sw128(sb + kB1 + o);
       umma::mma_bf16(d, al, bh, idesc, (acc || s > 0) ? 1u : 0u);
       umma::mma_bf16(d, ah, bl, idesc, 1u);

@@ -479,14 +479,24 @@ __global__ void __launch_bounds__(kXThreads, 1)
 
 // ---- step kernel -------------------------------------------------------------
 constexpr int kSThreads = 128;
-constexpr uint32_t kSB = 0;            // panel k-1 rows k0..k0+63 (B operand): 2 x 8 KB
-constexpr uint32_t kSAd = 16384;       // the same rows as an A operand (64 of 128 rows)
-constexpr uint32_t kSAo = 49152;       // the CTA's 128 rows of panel k-1
-constexpr uint32_t kSZero = 81920;     // zeros for the strip's bulk stores
+// Panel k-1 rows k0..k0+63: the B operand (region 0 at +0, region 1 at
+// +8 KB), and also the diagonal product's A operand (A1 = 8 KB: its rows
+// 64..127, whose accumulator lanes nobody reads, overlap what follows).
+constexpr uint32_t kSB = 0;
+constexpr uint32_t kSAo = 16384;       // the CTA's 128 rows of panel k-1: 2 x 16 KB
+constexpr uint32_t kSZero = 49152;     // zeros for the strip's bulk stores
 constexpr uint32_t kSZeroBytes = 4096;
 constexpr uint32_t kSDiag = kSZero + kSZeroBytes;
 constexpr uint32_t kSBar = kSDiag + (((uint32_t)sizeof(Diag64Smem) + 127u) & ~127u);
 constexpr uint32_t kSSmemBytes = kSBar + 64 + 1024;
+// Beside the outer-block update (n >= kWideMinN) two step CTAs share an SM
+// (shared memory and 2 x 128 TMEM columns), so a column's chunks need half
+// as many of the SMs it leaves free.  Below that the steps have the whole
+// GPU, and a larger request keeps each step CTA alone on its SM (neither a
+// second step CTA nor a look-ahead update CTA fits beside it): 1 x 8192 ran
+// 3286 us that way and 3769 us with the SMs shared.
+static_assert(2 * (kSSmemBytes + 1024) <= 228 * 1024, "two step CTAs per SM");
+constexpr uint32_t kSSmemAlone = 140 * 1024;
 constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the CTA's rows
 
 // Column k of every matrix, G CTAs per matrix.  P = base - X_{k-1} X_{k-1,kk}^T
@@ -496,7 +506,7 @@ constexpr uint32_t kSTmemCols = 128;   // [0, 64): diagonal rows; [64, 128): the
 // the CTA's 128-row chunks by forward substitution (one row per thread,
 // which is also one TMEM lane per thread), write L and the panel copy.
 template <int MODE>
-__global__ void __launch_bounds__(kSThreads, 1)
+__global__ void __launch_bounds__(kSThreads, 2)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
                       int32_t* __restrict__ info, const float* __restrict__ sig) {
@@ -551,12 +561,10 @@ __global__ void __launch_bounds__(kSThreads, 1)
       const uint32_t vr = own ? (uint32_t)min(kSThreads, n - r0) : 0u;
       if (tid == 0) {
         const size_t boff = panel_copy_row_byte(N, k - 1, k0);
-        umma::mbar_arrive_expect_tx(full, (first ? 4u * 8192u : 0u) + 2u * vr * 128u);
+        umma::mbar_arrive_expect_tx(full, (first ? 2u * 8192u : 0u) + 2u * vr * 128u);
         if (first) {
           umma::bulk_g2s(sm + kSB, W0 + boff, 8192u, full);
           umma::bulk_g2s(sm + kSB + 8192, W1 + boff, 8192u, full);
-          umma::bulk_g2s(sm + kSAd, W0 + boff, 8192u, full);
-          umma::bulk_g2s(sm + kSAd + 16384, W1 + boff, 8192u, full);
         }
         if (own) {
           const size_t aoff = panel_copy_row_byte(N, k - 1, r0);
@@ -566,7 +574,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
         if (umma::mbar_wait_bounded(full, ph_full, kSplitPolls)) {
           umma::fence_after_sync();
           const uint32_t sb = umma::smem_u32(sm + kSB);
-          if (first) panel_copy_mmas<MODE>(tmem, umma::smem_u32(sm + kSAd), sb, false);
+          if (first) panel_copy_mmas<MODE, 64, 8192u>(tmem, sb, sb, false);
           if (own) panel_copy_mmas<MODE>(tmem + 64, umma::smem_u32(sm + kSAo), sb, false);
         } else {
           *flag = 1;
@@ -839,7 +847,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
   const int sslot[3] = {kSlotSplitS0, kSlotSplitS1, kSlotSplitS2};
   const int wslot[3] = {kSlotSplitW0, kSlotSplitW1, kSlotSplitW2};
   if (int st = ensure_smem_attr((const void*)upd, kUSmemBytes, uslot[mi])) return st;
-  if (int st = ensure_smem_attr((const void*)stp, kSSmemBytes, sslot[mi])) return st;
+  if (int st = ensure_smem_attr((const void*)stp, kSSmemAlone, sslot[mi])) return st;
   float* sig = reinterpret_cast<float*>(copies + split_sig_offset(batch, n));
   if (m == B2P_MODE_FP8) {
     const int64_t blocks = batch * (n / 64);
@@ -857,12 +865,12 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     bw[0] = pb[1] + (size_t)batch * n * 64;
     bw[1] = bw[0] + (size_t)batch * n * nbw;
   }
-  // SMs the wide kernel may hold at once.
-  // SMs the wide kernel may hold at once: half while the chain of steps
-  // bounds the time (1 x 16384: 11.6 ms at 74 of 148 SMs, 15.3 ms at 40);
-  // two thirds once the outer-block updates do (1 x 32768: 56.0 ms at 100,
-  // 63.5 ms at 74).
-  const int64_t wide_ctas = std::max<int64_t>(1, n >= 24576 ? sms * 2 / 3 : sms / 2);
+  // SMs the wide kernel may hold at once: 9/16 while the chain of steps
+  // bounds the time, three quarters once the outer-block updates do.  Graph
+  // replay, FP8, with two step CTAs per SM: 1 x 16384 9.78 ms at 74 of 148
+  // SMs, 9.41 ms at 83, 9.80 ms at 92; 1 x 32768 47.1 ms at 98, 46.8 ms at
+  // 111, 46.6 ms at 86.
+  const int64_t wide_ctas = std::max<int64_t>(1, n >= 24576 ? sms * 3 / 4 : sms * 9 / 16);
 
   // Update of column k over panels [c0, c1) on stream `st`: P = base - sum,
   // split into about per_sm CTAs per SM.
@@ -921,8 +929,10 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_wide_kernel: %s", cudaGetErrorString(e));
     return B2P_OK;
   };
-  // Step CTAs of column k: one per SM, or per SM the wide kernel leaves free.
-  const int64_t step_sms = wide ? sms - wide_ctas : sms;
+  // Step CTAs of column k: two per SM on the SMs the wide kernel leaves
+  // free, else one per SM.
+  const int64_t step_sms = wide ? 2 * (sms - wide_ctas) : sms;
+  const uint32_t step_smem = wide ? kSSmemBytes : kSSmemAlone;
   auto step_G = [&](int k) -> int {
     const int chunks = (n - 64 * k - 64 + kSThreads - 1) / kSThreads;
     return (int)std::max<int64_t>(1, std::min<int64_t>(std::max(chunks, 1), step_sms / batch));
@@ -948,7 +958,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned)grid, 1, 1);
       cfg.blockDim = dim3(kSThreads, 1, 1);
-      cfg.dynamicSmemBytes = kSSmemBytes;
+      cfg.dynamicSmemBytes = step_smem;
       cfg.stream = s;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributePriority;
