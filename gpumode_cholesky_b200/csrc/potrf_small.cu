@@ -36,7 +36,7 @@ __device__ __forceinline__ void st_stream(float4* p, float4 v) {
                : "memory");
 }
 
-__global__ void __launch_bounds__(kWarp32Warps * 32, 8)
+__global__ void __launch_bounds__(kWarp32Warps * 32, 7)
     potrf_warp32_kernel(const float* __restrict__ a, float* __restrict__ l, MatrixList ml,
                         int32_t* __restrict__ info) {
   __shared__ __align__(16) float stage[kWarp32Warps][32 * kStageLd];

@@ -35,37 +35,43 @@ constexpr int kLtLd = 36;
 // L[k+1][k] = e / sqrt(d) itself and updates its column k+1 at once, so the
 // next pivot depends only on shuffles and registers.  The rest of the rank-1
 // update (columns k+2..31) goes through a double-buffered shared-memory copy
-// of column k, off that critical chain.  The arithmetic is the same as the
-// textbook right-looking update, value for value.
+// of column k and is deferred by one step: step k+1 applies it right after
+// shuffling out its own pivot, in the shadow of that pivot's reciprocal
+// square root.  The arithmetic is the same as the textbook right-looking
+// update, value for value and in the same order.
 __device__ __forceinline__ int warp_factor32(float (&x)[32], int lane, int w, float* colbuf,
                                              float& inv_pivot) {
   int bad = -1;
   inv_pivot = 1.0f;
+  float lprev = 0.0f;  // this lane's L[lane][k-1]
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
     if (k < w) {  // warp-uniform
       const float d = __shfl_sync(kFullMask, x[k], k);
       const float e = (k + 1 < 32) ? __shfl_sync(kFullMask, x[k], k + 1) : 0.0f;
-      if (bad < 0 && pivot_bad(d)) bad = k;
-      const float y = rsqrt_refined(d);
-      if (lane == k) inv_pivot = y;
-      x[k] = (lane == k) ? d * y : x[k] * y;
-      if (k + 1 < 32) x[k + 1] = fmaf(-x[k], e * y, x[k + 1]);
-      if (k + 2 < 32) {
-        float* cb = colbuf + (k & 1) * 32;
-        cb[lane] = x[k];
-        __syncwarp();
-        // x[j] -= L[lane][k] * L[j][k] for j > k + 1 (upper part is don't-care).
+      // Column k-1's update of columns k+1.. (column k had it by look-ahead).
+      if (k >= 1 && k + 1 < 32) {
+        const float* cb = colbuf + ((k - 1) & 1) * 32;
 #pragma unroll
-        for (int j4 = (k + 2) / 4; j4 < 8; ++j4) {
+        for (int j4 = (k + 1) / 4; j4 < 8; ++j4) {
           const float4 c = reinterpret_cast<const float4*>(cb)[j4];
           const float cv[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int j = 4 * j4 + q;
-            if (j > k + 1) x[j] = fmaf(-x[k], cv[q], x[j]);
+            if (j > k) x[j] = fmaf(-lprev, cv[q], x[j]);
           }
         }
+      }
+      if (bad < 0 && pivot_bad(d)) bad = k;
+      const float y = rsqrt_refined(d);
+      if (lane == k) inv_pivot = y;
+      x[k] = (lane == k) ? d * y : x[k] * y;
+      if (k + 1 < 32) x[k + 1] = fmaf(-x[k], e * y, x[k + 1]);
+      lprev = x[k];
+      if (k + 2 < 32) {
+        colbuf[(k & 1) * 32 + lane] = x[k];
+        __syncwarp();
       }
     }
   }
