@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kSymThreads) sym_kernel(const float* __restric
 constexpr int kBsThreads = 512;  // 16 warps: 8 x 4 register tiles over the 128 x 128 products
 constexpr int kBsLd = 132;                      // row stride of the three 128x128 buffers
 constexpr int kBsBuf = 128 * kBsLd;             // floats per buffer
-constexpr int kBsWork = 4 * 32 * 33;            // smem_trtri's work area
+constexpr int kBsWork = 64 * 64;                // trtri128's scratch W
 constexpr size_t kBsSmemBytes = sizeof(float) * (size_t)(3 * kBsBuf + kBsWork + 128 + 4);
 
 // acc[r][c] = sum_{k in [k0, k1)} X[k][8ti + r] * Y[k][4tj + c] (X, Y row-major
@@ -115,6 +115,107 @@ __device__ __forceinline__ void bs_tile(const float* X, const float* Y, int ti, 
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[r][c] = fmaf(xv[r], yv[c], acc[r][c]);
   }
+}
+
+// C = A B (NEG: -(A B)) for 64 x 64 blocks, with register tiles over the
+// 512 threads (2 rows x 4 columns each).  A and B are row-major in shared
+// memory; the K range of output column group c4 (4 columns) and row pair is
+// cut to where both operands can be non-zero: B lower triangular
+// (B[k][j] = 0 for k < j) when B_LOWER, A lower triangular (A[i][k] = 0 for
+// k > i) when A_LOWER.
+template <bool A_LOWER, bool B_LOWER, bool NEG>
+__device__ __forceinline__ void product64(const float* A, int lda, const float* B, int ldb, float* C, int ldc) {
+  const int t = threadIdx.x;
+  const int i0 = 2 * (t >> 4), j0 = 4 * (t & 15);  // rows i0, i0+1; columns j0..j0+3
+  float acc[2][4] = {};
+  const int k_lo = B_LOWER ? j0 : 0;
+  const int k_hi = A_LOWER ? i0 + 2 : 64;
+  for (int k = k_lo; k < k_hi; ++k) {
+    const float a0 = A[i0 * lda + k], a1 = A[(i0 + 1) * lda + k];
+    const float4 b = *reinterpret_cast<const float4*>(B + k * ldb + j0);
+    acc[0][0] = fmaf(a0, b.x, acc[0][0]);
+    acc[0][1] = fmaf(a0, b.y, acc[0][1]);
+    acc[0][2] = fmaf(a0, b.z, acc[0][2]);
+    acc[0][3] = fmaf(a0, b.w, acc[0][3]);
+    acc[1][0] = fmaf(a1, b.x, acc[1][0]);
+    acc[1][1] = fmaf(a1, b.y, acc[1][1]);
+    acc[1][2] = fmaf(a1, b.z, acc[1][2]);
+    acc[1][3] = fmaf(a1, b.w, acc[1][3]);
+  }
+  const float sg = NEG ? -1.0f : 1.0f;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+    *reinterpret_cast<float4*>(C + (i0 + r) * ldc + j0) =
+        make_float4(sg * acc[r][0], sg * acc[r][1], sg * acc[r][2], sg * acc[r][3]);
+}
+
+// The same for two independent 32 x 32 products at once: block h = t / 256
+// reads A + h a_off and B + h b_off and writes C + h c_off; each thread
+// computes 1 row x 4 columns.
+template <bool A_LOWER, bool B_LOWER, bool NEG>
+__device__ __forceinline__ void product32x2(const float* A, int lda, const float* B, int ldb, float* C, int ldc,
+                                                int a_off, int b_off, int c_off) {
+  const int t = threadIdx.x;
+  const int h = t >> 8, u = t & 255;
+  const int i = u >> 3, j0 = 4 * (u & 7);
+  const float* Ah = A + h * a_off;
+  const float* Bh = B + h * b_off;
+  float acc[4] = {};
+  const int k_lo = B_LOWER ? j0 : 0;
+  const int k_hi = A_LOWER ? i + 1 : 32;
+  for (int k = k_lo; k < k_hi; ++k) {
+    const float a = Ah[i * lda + k];
+    const float4 b = *reinterpret_cast<const float4*>(Bh + k * ldb + j0);
+    acc[0] = fmaf(a, b.x, acc[0]);
+    acc[1] = fmaf(a, b.y, acc[1]);
+    acc[2] = fmaf(a, b.z, acc[2]);
+    acc[3] = fmaf(a, b.w, acc[3]);
+  }
+  const float sg = NEG ? -1.0f : 1.0f;
+  *reinterpret_cast<float4*>(C + h * c_off + i * ldc + j0) = make_float4(sg * acc[0], sg * acc[1], sg * acc[2], sg * acc[3]);
+}
+
+// U = L^{-1} of the 128 x 128 lower-triangular L in shared memory (row stride
+// ld), into U (row stride ld, zero above the diagonal), by block recursion:
+//   32 x 32 diagonal blocks by forward substitution (warp b, lane = column);
+//   U_10 = -U_11 (L_10 U_00) inside each 64-block (both 64-blocks at once);
+//   U_21 = -U_22 (L_21 U_11) for the 64-blocks.
+// invd holds 1 / L_ii; W is scratch of 64 x kBsWLd floats.  All 512 threads.
+constexpr int kBsWLd = 64;
+static_assert(64 * kBsWLd <= kBsWork, "trtri128 scratch fits the work area");
+__device__ void trtri128(const float* L, float* U, int ld, const float* invd, float* W) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < 128 * ld; e += kBsThreads) U[e] = 0.0f;
+  __syncthreads();
+  if (warp < 4) {
+    const int kb = 32 * warp, c = lane;
+    float x[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) x[j] = (j == c) ? 1.0f : 0.0f;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      x[m] *= invd[kb + m];
+#pragma unroll
+      for (int j = m + 1; j < 32; ++j) x[j] = fmaf(-L[(kb + j) * ld + kb + m], x[m], x[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j >= c) U[(kb + j) * ld + kb + c] = x[j];
+  }
+  __syncthreads();
+  // Inside each 64-block h: W_h = L_10 U_00 (W rows 32 h ..), then U_10 = -U_11 W_h.
+  // Block h covers rows / columns 64 h .. 64 h + 63; its L_10 starts at
+  // (64 h + 32, 64 h), U_00 at (64 h, 64 h), U_11 at (64 h + 32, 64 h + 32).
+  product32x2<false, true, false>(L + 32 * ld, ld, U, ld, W, kBsWLd, 64 * (ld + 1), 64 * (ld + 1), 32 * kBsWLd);
+  __syncthreads();
+  product32x2<true, false, true>(U + 32 * ld + 32, ld, W, kBsWLd, U + 32 * ld, ld, 64 * (ld + 1), 32 * kBsWLd,
+                                 64 * (ld + 1));
+  __syncthreads();
+  // W = L_21 U_11 (the first 64-block's inverse), then U_21 = -U_22 W.
+  product64<false, true, false>(L + 64 * ld, ld, U, ld, W, kBsWLd);
+  __syncthreads();
+  product64<true, false, true>(U + 64 * ld + 64, ld, W, kBsWLd, U + 64 * ld, ld);
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kBsThreads, 1)
@@ -158,8 +259,7 @@ __global__ void __launch_bounds__(kBsThreads, 1)
         bB[j * kBsLd + i] = v;
       }
     // U = L^{-1} into bC.
-    smem_trtri<kBsThreads>(bA, 128, kBsLd, bC, kBsLd, sc, work);
-    __syncthreads();
+    trtri128(bA, bC, kBsLd, sc.invd, work);
     // Z = P U: Z[i][j] = sum_k P^T[k][i] U[k][j], k in [j, i] (lower tiles).
     if (lower) bs_tile(bB, bC, ti, tj, 4 * tj, 8 * ti + 8, acc);
     __syncthreads();

@@ -948,7 +948,8 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
     if (k >= 2) {
       if (int st = check(cudaStreamWaitEvent(s, side->join[k & 1], 0), "cudaStreamWaitEvent")) return st;
     }
-    // Step (with the newest panel k-1): one CTA per SM in total.
+    // Step (with the newest panel k-1): step_ctas(k) CTAs, one 128-row
+    // chunk each where the SMs allow.
     const int G = step_G(k);
     const int grid = (int)step_ctas(k);
     {

@@ -8,9 +8,6 @@
 //    shared memory, blocked by 32: warp 0 factors the diagonal block, every
 //    thread solves one panel row against it, then 4x4 register tiles apply
 //    the rank-32 trailing update to the lower triangle.
-//  * smem_trtri:    in-place-safe inverse of the lower-triangular factor in
-//    shared memory (n <= 128), blocked by 32; used by the blocked path to
-//    turn the panel TRSM into a GEMM.
 //
 // The algorithm is the textbook right-looking Cholesky that LAPACK's potrf
 // (called by the reference's ref_kernel, reference/reference.py:129-130, and
@@ -78,7 +75,7 @@ __device__ __forceinline__ int warp_factor32(float (&x)[32], int lane, int w, fl
   return bad;
 }
 
-// Scratch layout for smem_potrf / smem_trtri (floats).
+// Scratch layout for smem_potrf (floats).
 struct TileScratch {
   float* lt;      // [32][kLtLd]   transposed L of the current diagonal block
   float* invd;    // [128]         1/L[i][i]
@@ -231,78 +228,6 @@ __device__ int smem_potrf(float* S, int n, int lds, const TileScratch& sc) {
   }
   __syncthreads();
   return *sc.flag;
-}
-
-// Inverse T = L^{-1} of the lower-triangular n x n factor in S (row stride
-// lds), written to Tm (row stride ldt, lower triangle + zero upper).  Uses
-// sc.invd from the preceding smem_potrf.  n <= 128, NT >= 128.
-//   diagonal 32-blocks: lane c of warp b forward-substitutes column c;
-//   off-diagonal blocks by block distance d: T_ij = -T_ii * sum_k L_ik T_kj.
-template <int NT>
-__device__ void smem_trtri(const float* S, int n, int lds, float* Tm, int ldt,
-                           const TileScratch& sc, float* work /* [4][32][33] */) {
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int warp = tid >> 5;
-  const int nblk = (n + 31) / 32;
-  // Zero the whole target first (upper part and padding stay zero).
-  for (int e = tid; e < n * ldt; e += NT) Tm[e] = 0.0f;
-  __syncthreads();
-  if (warp < nblk) {
-    const int kb = warp * 32;
-    const int w = min(32, n - kb);
-    const int c = lane;
-    float x[32];
-#pragma unroll
-    for (int j = 0; j < 32; ++j) x[j] = (j == c) ? 1.0f : 0.0f;
-#pragma unroll
-    for (int m = 0; m < 32; ++m) {
-      if (m < w) {
-        x[m] *= sc.invd[kb + m];
-#pragma unroll
-        for (int j = m + 1; j < 32; ++j) {
-          if (j < w) x[j] = fmaf(-S[(size_t)(kb + j) * lds + kb + m], x[m], x[j]);
-        }
-      }
-    }
-    if (c < w) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (j < w && j >= c) Tm[(size_t)(kb + j) * ldt + kb + c] = x[j];
-    }
-  }
-  __syncthreads();
-  for (int d = 1; d < nblk; ++d) {
-    // W_(ib) = sum_{k=jb}^{ib-1} L_(ib,k) T_(k,jb) for every pair at distance d.
-    const int npairs = nblk - d;
-    for (int e = tid; e < npairs * 1024; e += NT) {
-      const int p = e >> 10;
-      const int r = (e >> 5) & 31;
-      const int cc = e & 31;
-      const int jb = p, ib = p + d;
-      const int i = ib * 32 + r, j = jb * 32 + cc;
-      float s = 0.0f;
-      if (i < n && j < n) {
-        const int kend = ib * 32;
-        for (int k = jb * 32; k < kend; ++k) s = fmaf(S[(size_t)i * lds + k], Tm[(size_t)k * ldt + j], s);
-      }
-      work[(p * 32 + r) * 33 + cc] = s;
-    }
-    __syncthreads();
-    for (int e = tid; e < npairs * 1024; e += NT) {
-      const int p = e >> 10;
-      const int r = (e >> 5) & 31;
-      const int cc = e & 31;
-      const int jb = p, ib = p + d;
-      const int i = ib * 32 + r, j = jb * 32 + cc;
-      if (i < n && j < n) {
-        float s = 0.0f;
-        for (int k = 0; k <= r; ++k) s = fmaf(Tm[(size_t)i * ldt + ib * 32 + k], work[(p * 32 + k) * 33 + cc], s);
-        Tm[(size_t)i * ldt + j] = -s;
-      }
-    }
-    __syncthreads();
-  }
 }
 
 }  // namespace b2p
