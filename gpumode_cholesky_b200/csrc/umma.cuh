@@ -178,7 +178,7 @@ __device__ __forceinline__ void mbar_arrive_cluster(uint64_t* local, uint32_t ra
                : "memory");
 }
 
-// ---- bulk copies (untiled TMA, no multicast) -------------------------------
+// ---- bulk copies (untiled TMA, each into this CTA's own shared memory) ----
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
                : "memory");
