@@ -239,6 +239,13 @@ __device__ __forceinline__ int diag64_factor(Diag64Smem& sm, Bar bar = Bar()) {
   return b0 >= 0 ? b0 : (b1 >= 0 ? 32 + b1 : -1);
 }
 
+// diag64_factor's result as every thread of the CTA can read it back once
+// the factorization's last barrier has been passed by all of them.
+__device__ __forceinline__ int diag64_status(const Diag64Smem& sm) {
+  if (sm.err) return kDiagTimeout;
+  return sm.bad[0] >= 0 ? sm.bad[0] : (sm.bad[1] >= 0 ? 32 + sm.bad[1] : -1);
+}
+
 // Column c of L^{-1} for a 32x32 lower L given as lt = L^T (row stride LD)
 // and invd = 1/diag: forward substitution L y = e_c in right-looking order.
 template <int LD>

@@ -12,8 +12,9 @@
 //               copies (cp.async.bulk, two stages) and issues the MMAs;
 //   2. panel    P = A[k0:n, k0:k0+64] - D (A read from HBM exactly once);
 //               the top 64x64 block is factored and inverted in shared memory
-//               (diag64.cuh) and the rows below are solved as X = P T^T
-//               (FP32 SIMT, T = L_kk^{-1});
+//               (diag64.cuh, warps 0-3) while warps 4-7 form P of the later
+//               row tiles and park it in TMEM in place of D; the rows below
+//               are solved as X = P T^T (FP32 SIMT, T = L_kk^{-1});
 //   3. output   L_kk, X and the zero strip above go to L (written once);
 //               X's tensor-core copy (BF16 hi and lo, or TF32 halves) goes to
 //               the workspace for the updates of later block columns.
@@ -55,6 +56,37 @@ constexpr uint32_t kFZeroOff = kFUnion + 128;  // zeros, source of the strip's b
 constexpr uint32_t kFZeroBytes = 4096;           // >= 4 (n - 64) bytes for n <= 1024
 constexpr uint32_t kFSmemBytes = kFZeroOff + kFZeroBytes + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
+
+constexpr uint32_t kNoTmem = 0xffffffffu;
+
+// One thread's 32 values of P = A - D for row r0 + rl (rl < 0: beyond the
+// matrix, zeros) and columns k0 + 32 h .. + 31, D from the TMEM columns at
+// dcol (lanes of warp quarter w4; kNoTmem: no update yet).  The TMEM load is
+// warp-collective, so every lane of the warp calls this.
+__device__ __forceinline__ void p_form(float (&p)[32], const float* A, int n, int k0, int r0, int rl, int w4, int h,
+                                       uint32_t dcol) {
+  float d[32];
+  if (dcol != kNoTmem) {
+    umma::tmem_ld32(dcol + ((uint32_t)(32 * w4) << 16), d);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) d[q] = 0.0f;
+  }
+  if (rl >= 0) {
+    const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + 32 * h);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 v = src[q];
+      p[4 * q + 0] = v.x - d[4 * q + 0];
+      p[4 * q + 1] = v.y - d[4 * q + 1];
+      p[4 * q + 2] = v.z - d[4 * q + 2];
+      p[4 * q + 3] = v.w - d[4 * q + 3];
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) p[q] = 0.0f;
+  }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
@@ -194,27 +226,12 @@ __global__ void __launch_bounds__(kFThreads, 2)
         {
           const int w4 = warp & 3, h = warp >> 2;
           const int rl = 32 * w4 + lane;
-          float d[32];
-          if (k > 0) {
-            umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kFB * mt + 32 * h), d);
-          } else {
-#pragma unroll
-            for (int q = 0; q < 32; ++q) d[q] = 0.0f;
-          }
           float p[32];
-          if (rl < vr) {
-            const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + 32 * h);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const float4 v = src[q];
-              p[4 * q + 0] = v.x - d[4 * q + 0];
-              p[4 * q + 1] = v.y - d[4 * q + 1];
-              p[4 * q + 2] = v.z - d[4 * q + 2];
-              p[4 * q + 3] = v.w - d[4 * q + 3];
-            }
+          if (mt > 0) {
+            // Formed during the diagonal phase (below) and kept in TMEM.
+            umma::tmem_ld32(tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kFB * mt + 32 * h), p);
           } else {
-#pragma unroll
-            for (int q = 0; q < 32; ++q) p[q] = 0.0f;
+            p_form(p, A, n, k0, r0, rl < vr ? rl : -1, w4, h, k > 0 ? tmem + (uint32_t)(32 * h) : kNoTmem);
           }
 #pragma unroll
           for (int q = 0; q < 32; ++q) PtT[(32 * h + q) * kFPtLd + rl] = p[q];
@@ -226,8 +243,31 @@ __global__ void __launch_bounds__(kFThreads, 2)
         umma::fence_before_sync();
         __syncthreads();
         if (mt == 0) {
-          // L_kk and T^T (T = L_kk^{-1}, in dg.T) from the pipelined engine.
-          const int bad = diag64_factor_invert(dg);
+          // L_kk and T^T (T = L_kk^{-1}, in dg.T) from the pipelined engine
+          // on warps 0-3.  Meanwhile warps 4-7 form P = A - D of the later
+          // row tiles (their loads of A hide behind the diagonal engine) and
+          // park it in place of D in TMEM, each warp its lane quarter.
+          if (warp < 4) {
+            diag64_factor_invert(dg, NamedBarrier1<kD64Threads>());
+          } else {
+            const int w4 = warp & 3;
+            for (int mt2 = 1; mt2 < mtiles; ++mt2) {
+              const int r2 = k0 + mt2 * kFM, v2 = min(kFM, n - r2);
+              const int rl = 32 * w4 + lane;
+#pragma unroll 1
+              for (int h = 0; h < 2; ++h) {
+                const uint32_t col = tmem + (uint32_t)(kFB * mt2 + 32 * h);
+                float p[32];
+                p_form(p, A, n, k0, r2, rl < v2 ? rl : -1, w4, h, k > 0 ? col : kNoTmem);
+                umma::tmem_st32(col + ((uint32_t)(32 * w4) << 16), p);
+              }
+            }
+            umma::tmem_wait_st();
+          }
+          umma::fence_before_sync();
+          __syncthreads();
+          umma::fence_after_sync();
+          const int bad = diag64_status(dg);
           if (bad == kDiagTimeout) {
             ok = false;
             break;
