@@ -47,6 +47,15 @@ struct NamedBarrier1 {
   }
 };
 
+// The same over barrier 2 (a second group of warps that runs its own
+// barrier 1 at the same time must not share the id).
+template <int NTHREADS>
+struct NamedBarrier2 {
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync 2, %0;" ::"n"(NTHREADS) : "memory");
+  }
+};
+
 struct Diag64Smem {
   float S[64 * kD64Ld];   // block: A in, L out (lower part)
   float T[64 * kD64Ld];   // diag64_factor_invert: T^T, T = L^{-1} (T[c][j] = L^{-1}[j][c])

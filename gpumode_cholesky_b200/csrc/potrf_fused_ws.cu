@@ -11,7 +11,10 @@
 //   warps 0-7 (consumers)  per tile: wait `acc_ready`, read D from TMEM
 //        (then arrive `acc_free`), P = A - D, factor + invert the diagonal
 //        block (tile 0), X = P T^T in FP32, write L and the tensor-core copy
-//        of X, then publish the tile's completion count.
+//        of X, then publish the tile's completion count.  While warps 0-3
+//        factor the diagonal block, warps 4-7 form P of the CTA's later
+//        tiles and park it in their TMEM slots (released, as before, when
+//        each tile is processed).
 //
 // Small batches run as clusters of CL = 2, 4 or 8 CTAs per matrix: rank r
 // takes the row tiles t = r (mod CL) of every block column (tile 0 holds the
@@ -261,15 +264,19 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
         const bool diag_only = CL > 1 && rank != 0 && mt == 0;
         const int r0 = k0 + mt * kWM;
         const int vr = diag_only ? 64 : min(kWM, n - r0);
-        // (a) D from TMEM, P = A - D.
+        // (a) D from TMEM, P = A - D.  Tiles after the first were formed
+        // during the diagonal phase (b) and hold P in their TMEM slot.
+        const bool preformed = k > 0 && j > 0;
         {
           const int w4 = warp & 3, h = warp >> 2;
           const int rl = 32 * w4 + lane;
           float d[32];
           if (k > 0) {
-            const bool got = ws_wait(br.acc_ready + j, (ready_par >> j) & 1u, br.flag);
+            if (!preformed) {
+              const bool got = ws_wait(br.acc_ready + j, (ready_par >> j) & 1u, br.flag);
+              if (!got) *br.flag = 1;
+            }
             ready_par ^= 1u << j;
-            if (!got) *br.flag = 1;
           }
           cbar();
           if (*br.flag) {
@@ -287,7 +294,10 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
             for (int q = 0; q < 32; ++q) d[q] = 0.0f;
           }
           float p[32];
-          if (rl < vr) {
+          if (preformed) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) p[q] = d[q];
+          } else if (rl < vr) {
             const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r0 + rl) * n + k0 + 32 * h);
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -313,8 +323,53 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
         cbar();
         // (b) diagonal block: L_kk and T^T (pipelined engine), zero strip.
         if (mt == 0) {
-          const int bad = diag64_factor_invert(dg, cbar);
-          if (bad == kDiagTimeout) {
+          // Warps 0-3 run the diagonal engine.  Warps 4-7 meanwhile form
+          // P = A - D of this CTA's later tiles of the column (each warp its
+          // TMEM lane quarter, both column halves) and store it in place of D;
+          // their slots are released when those tiles are processed below.
+          if (warp < 4) {
+            diag64_factor_invert(dg, NamedBarrier2<kD64Threads>());
+          } else if (k > 0) {
+            const int w4 = warp & 3;
+            const int rl = 32 * w4 + lane;
+            for (int j2 = 1; j2 < nt; ++j2) {
+              const int mt2 = ws_tile_of<CL>(j2, rank);
+              const int r2 = k0 + mt2 * kWM, v2 = min(kWM, n - r2);
+              const bool got = ws_wait(br.acc_ready + j2, (ready_par >> j2) & 1u, br.flag);
+              if (!__all_sync(0xffffffffu, got)) {
+                *br.flag = 1;
+                break;
+              }
+              umma::fence_after_sync();
+#pragma unroll 1
+              for (int h = 0; h < 2; ++h) {
+                const uint32_t taddr = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(kWB * j2 + 32 * h);
+                float d[32], p[32];
+                umma::tmem_ld32(taddr, d);
+                if (rl < v2) {
+                  const float4* src = reinterpret_cast<const float4*>(A + (size_t)(r2 + rl) * n + k0 + 32 * h);
+#pragma unroll
+                  for (int q = 0; q < 8; ++q) {
+                    const float4 v = src[q];
+                    p[4 * q + 0] = v.x - d[4 * q + 0];
+                    p[4 * q + 1] = v.y - d[4 * q + 1];
+                    p[4 * q + 2] = v.z - d[4 * q + 2];
+                    p[4 * q + 3] = v.w - d[4 * q + 3];
+                  }
+                } else {
+#pragma unroll
+                  for (int q = 0; q < 32; ++q) p[q] = 0.0f;
+                }
+                umma::tmem_st32(taddr, p);
+              }
+            }
+            umma::tmem_wait_st();
+          }
+          umma::fence_before_sync();
+          cbar();
+          umma::fence_after_sync();
+          const int bad = diag64_status(dg);
+          if (bad == kDiagTimeout || *br.flag) {
             failed = true;
             if (tid == 0) *br.flag = 1;  // the producer gives up too
           }
