@@ -58,6 +58,7 @@ constexpr uint32_t kFSmemBytes = kFZeroOff + kFZeroBytes + 1024;
 constexpr uint32_t kFSmemOneCta = 120 * 1024;  // forces one CTA per SM (512 TMEM columns)
 
 constexpr uint32_t kNoTmem = 0xffffffffu;
+constexpr int kFStripThread = 128;  // warp 4, free during the diagonal engine
 
 // One thread's 32 values of P = A - D for row r0 + rl (rl < 0: beyond the
 // matrix, zeros) and columns k0 + 32 h .. + 31, D from the TMEM columns at
@@ -250,6 +251,14 @@ __global__ void __launch_bounds__(kFThreads, 2)
           if (warp < 4) {
             diag64_factor_invert(dg, NamedBarrier1<kD64Threads>());
           } else {
+            // Zero strip right of the diagonal block: one bulk store per row
+            // from the zero buffer, issued by one thread and left to run.
+            const uint32_t strip = 4u * (uint32_t)(n - k0 - kFB);
+            if (tid == kFStripThread && strip > 0) {
+              for (int r = 0; r < 64; ++r)
+                umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kFB, sm + kFZeroOff, strip);
+              umma::bulk_commit();
+            }
             const int w4 = warp & 3;
             for (int mt2 = 1; mt2 < mtiles; ++mt2) {
               const int r2 = k0 + mt2 * kFM, v2 = min(kFM, n - r2);
@@ -281,14 +290,6 @@ __global__ void __launch_bounds__(kFThreads, 2)
                                    c + 3 <= r ? srow[3] : 0.f);
             *reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + c) = v;
           }
-          // Zero strip right of the diagonal block: one bulk store per row from
-          // the zero buffer, issued by one thread and left to run.
-          const uint32_t strip = 4u * (uint32_t)(n - k0 - kFB);
-          if (tid == 0 && strip > 0) {
-            for (int r = 0; r < 64; ++r)
-              umma::bulk_s2g(L + (size_t)(k0 + r) * n + k0 + kFB, sm + kFZeroOff, strip);
-            umma::bulk_commit();
-          }
           __syncthreads();
         }
         // X = P T^T for the rows below the diagonal block (triangle skipped),
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
   }
   // The strip's bulk stores read the zero buffer until they complete.
-  if (tid == 0) umma::bulk_wait_all();
+  if (tid == kFStripThread) umma::bulk_wait_all();
   // Release TMEM after a last bounded chance for outstanding MMAs.
   if (!ok) {
     umma::mbar_wait_bounded(done, ph_done, kFPolls);

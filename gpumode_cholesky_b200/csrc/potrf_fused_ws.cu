@@ -68,6 +68,7 @@ constexpr int kWMaxSlots = 8;                   // TMEM accumulator slots (512 c
 constexpr uint32_t kWSmemBytes = kWCntOff + 4 * kWMaxTiles + 1024;
 
 using ConsumerBar = NamedBarrier1<kWConsumers>;
+constexpr int kWStripThread = 128;  // consumer warp 4, free during the diagonal engine
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(mbar)) : "memory");
@@ -329,7 +330,20 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           // their slots are released when those tiles are processed below.
           if (warp < 4) {
             diag64_factor_invert(dg, NamedBarrier2<kD64Threads>());
-          } else if (k > 0) {
+          } else {
+            // Zero strip right of the diagonal block: one bulk store per row
+            // from the zero buffer, issued by one thread and left to run.
+            const uint32_t strip = 4u * (uint32_t)(n - k0 - kWB);
+            if (tid == kWStripThread && rank == 0 && strip > 0) {
+              for (int r = 0; r < 64; ++r) {
+                uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + kWB);
+                for (uint32_t off = 0; off < strip; off += kWZeroBytes)
+                  umma::bulk_s2g(row + off, zeros, min(kWZeroBytes, strip - off));
+              }
+              umma::bulk_commit();
+            }
+          }
+          if (warp >= 4 && k > 0) {
             const int w4 = warp & 3;
             const int rl = 32 * w4 + lane;
             for (int j2 = 1; j2 < nt; ++j2) {
@@ -381,17 +395,6 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
                                          c + 2 <= r ? srow[2] : 0.f, c + 3 <= r ? srow[3] : 0.f);
             *reinterpret_cast<float4*>(L + (size_t)(k0 + r) * n + k0 + c) = v;
           }
-          // Zero strip right of the diagonal block: one bulk store per row from
-          // the zero buffer, issued by one thread and left to run.
-          const uint32_t strip = 4u * (uint32_t)(n - k0 - kWB);
-          if (tid == 0 && rank == 0 && strip > 0) {
-            for (int r = 0; r < 64; ++r) {
-              uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + kWB);
-              for (uint32_t off = 0; off < strip; off += kWZeroBytes)
-                umma::bulk_s2g(row + off, zeros, min(kWZeroBytes, strip - off));
-            }
-            umma::bulk_commit();
-          }
           cbar();
         }
         if (diag_only) continue;
@@ -432,7 +435,7 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
     if (failed) break;
   }
   // The strip's bulk stores read the zero buffer until they complete.
-  if (tid == 0) umma::bulk_wait_all();
+  if (tid == kWStripThread) umma::bulk_wait_all();
 }
 
 template <int MODE, int CL>
