@@ -479,6 +479,7 @@ __global__ void __launch_bounds__(kXThreads, 1)
 
 // ---- step kernel -------------------------------------------------------------
 constexpr int kSThreads = 128;
+constexpr int kSStripThread = 96;  // warp 3 lane 0
 // Panel k-1 rows k0..k0+63: the B operand (region 0 at +0, region 1 at
 // +8 KB), and also the diagonal product's A operand (A1 = 8 KB: its rows
 // 64..127, whose accumulator lanes nobody reads, overlap what follows).
@@ -596,6 +597,20 @@ __global__ void __launch_bounds__(kSThreads, 2)
       if (tid == 0 && info != nullptr) info[b] = -1;
       break;
     }
+    // 2. Zero strip right of the diagonal block: rows g, g + G, ... of it as
+    //    bulk stores from the zero buffer, issued by warp 3 (idle in the
+    //    P_kk formation and the diagonal factor) and left to run.
+    if (tid == kSStripThread) {
+      const uint32_t strip = 4u * (uint32_t)(n - k0 - 64);
+      if (strip > 0) {
+        for (int r = g; r < 64; r += G) {
+          uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + 64);
+          for (uint32_t off = 0; off < strip; off += kSZeroBytes)
+            umma::bulk_s2g(row + off, sm + kSZero, min(kSZeroBytes, strip - off));
+        }
+        umma::bulk_commit();
+      }
+    }
     if (warp < 2) {
       const float4* src = reinterpret_cast<const float4*>(base + (size_t)(k0 + tid) * bld);
       float4* dst = reinterpret_cast<float4*>(dg.S + tid * kD64Ld);
@@ -636,19 +651,6 @@ __global__ void __launch_bounds__(kSThreads, 2)
           info[b] = bad >= 0 ? bad + 1 : 0;
         else if (bad >= 0 && info[b] == 0)
           info[b] = k0 + bad + 1;
-      }
-    }
-    // 2. Zero strip right of the diagonal block: rows g, g + G, ... of it as
-    //    bulk stores from the zero buffer.
-    if (tid == 0) {
-      const uint32_t strip = 4u * (uint32_t)(n - k0 - 64);
-      if (strip > 0) {
-        for (int r = g; r < 64; r += G) {
-          uint8_t* row = reinterpret_cast<uint8_t*>(L + (size_t)(k0 + r) * n + k0 + 64);
-          for (uint32_t off = 0; off < strip; off += kSZeroBytes)
-            umma::bulk_s2g(row + off, sm + kSZero, min(kSZeroBytes, strip - off));
-        }
-        umma::bulk_commit();
       }
     }
     // 3. Panel rows: X L_kk^T = P, one row (and one TMEM lane) per thread.
@@ -709,7 +711,7 @@ __global__ void __launch_bounds__(kSThreads, 2)
   }
   if (!ok) umma::mbar_wait_bounded(done, ph_done, kSplitPolls);
   // The strip's bulk stores read the zero buffer until they complete.
-  if (tid == 0) umma::bulk_wait_all();
+  if (tid == kSStripThread) umma::bulk_wait_all();
   umma::fence_before_sync();
   __syncthreads();
   if (upd && warp == 0) umma::tmem_dealloc(tmem, kSTmemCols);
