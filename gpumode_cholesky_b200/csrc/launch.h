@@ -141,6 +141,7 @@ enum KernelId {
   kKGpForward,
   kKGpLbar,
   kKRescue,
+  kKAudit,
   kKCount
 };
 

@@ -1,17 +1,21 @@
 // Pivot audit and FP32 rescue of the pivot guard (guard.cuh).
 //
 // Right after a tensor-mode path (potrf_fused.cu, potrf_fused_ws.cu,
-// potrf_split.cu) has factored a batch, on the same stream, this kernel
-//   1. audits every matrix's computed pivots L_jj^2 against the mode's
-//      bound and writes the first failing block column per matrix, or -1,
-//      into the guard state (matrices dealt round-robin to the CTAs; one
-//      strided pass over the diagonals of A and L);
-//   2. after a grid barrier, returns when no matrix failed (the usual case);
-//   3. otherwise refactors every failing matrix from its first column in
-//      plain FP32 and overwrites its L and info; the others are not touched.
+// potrf_split.cu) has factored a batch, on the same stream, two launches:
+//   1. guard_audit_kernel audits every matrix's computed pivots L_jj^2
+//      against the mode's bound and writes the first failing block column
+//      per matrix, or -1, into the guard state (contiguous matrix ranges per
+//      CTA; one strided pass over the diagonals of A and L); it also resets
+//      the rescue's grid barrier;
+//   2. potrf_rescue_kernel reads the guard state and returns when no matrix
+//      failed (the usual case); otherwise it refactors every failing matrix
+//      from its first column in plain FP32 and overwrites its L and info;
+//      the others are not touched.
+// The kernel boundary between them is the audit's grid-wide barrier, so the
+// usual case waits on no spin.
 //
-// Schedule: one cooperative launch, one CTA per SM (all CTAs resident at
-// once), left-looking by 64-wide block columns.  In column k the jobs are
+// Rescue schedule: one cooperative launch, one CTA per SM (all CTAs
+// resident at once), left-looking by 64-wide block columns.  In column k the jobs are
 // (flagged matrix, 128-row chunk of the rows below the diagonal block); each
 // job recomputes the diagonal block's P = A - L[:, 0:k0] L[k-block, 0:k0]^T
 // in FP32 (guard_row_p), factors it with the diagonal engine (diag64_factor),
@@ -72,27 +76,19 @@ __device__ __forceinline__ bool rescue_grid_sync(int* bar, int* s_ok) {
   return *s_ok != 0;
 }
 
-__global__ void __launch_bounds__(kRThreads, 1)
-    potrf_rescue_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n, int mode,
-                        int32_t* __restrict__ gstate, int* bar, int32_t* __restrict__ info) {
-  extern __shared__ unsigned char rraw[];
-  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(rraw) + 127) & ~(uintptr_t)127);
-  Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kRDiagOff);
-  float* stage = reinterpret_cast<float*>(sm + kRStageOff);
-  float* rows = reinterpret_cast<float*>(sm + kRRowsOff);
-  int64_t* list = reinterpret_cast<int64_t*>(sm + kRListOff);
-  int* misc = reinterpret_cast<int*>(sm + kRMiscOff);  // [0] list size, [1] barrier verdict, [4..7] warp counts
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int N = n / 64;
+// The audit (step 1 above): the first block column whose pivot fails, per
+// matrix.  Each CTA takes a contiguous range of matrices, its threads stride
+// over all their (matrix, pivot) pairs at once, and the first failing column
+// of each matrix is an atomic minimum in shared memory (in rounds of
+// 2 kRList matrices when the range is longer).
+__global__ void __launch_bounds__(kRThreads)
+    guard_audit_kernel(const float* __restrict__ a, const float* __restrict__ l, int64_t batch, int n, int mode,
+                       int32_t* __restrict__ gstate, int* bar) {
+  __shared__ int first[2 * kRList];
+  const int tid = threadIdx.x;
   const size_t n2 = (size_t)n * n;
-
-  // 1. Audit: the first block column whose pivot fails, per matrix.  Each
-  //    CTA takes a contiguous range of matrices, its threads stride over all
-  //    their (matrix, pivot) pairs at once, and the first failing column of
-  //    each matrix is an atomic minimum in shared memory (the list area,
-  //    kRList * 2 ints, in rounds when the range is longer).
+  if (blockIdx.x == 0 && tid == 0) bar[0] = bar[1] = 0;  // the rescue's grid barrier
   {
-    int* first = reinterpret_cast<int*>(list);
     const int64_t per = (batch + gridDim.x - 1) / gridDim.x;
     const int64_t lo0 = per * (int64_t)blockIdx.x;
     const int64_t lo = lo0 < batch ? lo0 : batch, hi = lo + per < batch ? lo + per : batch;
@@ -130,11 +126,21 @@ __global__ void __launch_bounds__(kRThreads, 1)
       __syncthreads();
     }
   }
-  if (!rescue_grid_sync(bar, misc + 1)) {
-    if (tid == 0 && info != nullptr)
-      for (int64_t b = blockIdx.x; b < batch; b += gridDim.x) info[b] = -1;
-    return;
-  }
+}
+
+__global__ void __launch_bounds__(kRThreads, 1)
+    potrf_rescue_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n, int mode,
+                        int32_t* __restrict__ gstate, int* bar, int32_t* __restrict__ info) {
+  extern __shared__ unsigned char rraw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(rraw) + 127) & ~(uintptr_t)127);
+  Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kRDiagOff);
+  float* stage = reinterpret_cast<float*>(sm + kRStageOff);
+  float* rows = reinterpret_cast<float*>(sm + kRRowsOff);
+  int64_t* list = reinterpret_cast<int64_t*>(sm + kRListOff);
+  int* misc = reinterpret_cast<int*>(sm + kRMiscOff);  // [0] list size, [1] barrier verdict, [4..7] warp counts
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N = n / 64;
+  const size_t n2 = (size_t)n * n;
 
   // 2. Fast exit: nothing flagged (the usual case).
   bool any = false;
@@ -235,8 +241,11 @@ __global__ void __launch_bounds__(kRThreads, 1)
 int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, int* bar, int32_t* info,
                  cudaStream_t s) {
   if (batch == 0) return B2P_OK;
-  cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(int), s);
-  if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "cudaMemsetAsync(rescue barrier): %s", cudaGetErrorString(e));
+  {
+    TraceScope ts(kKAudit, s);
+    guard_audit_kernel<<<(unsigned)device_sms(), kRThreads, 0, s>>>(a, l, batch, n, mode, gstate, bar);
+    if (int st = check_launch("guard_audit_kernel")) return st;
+  }
   if (int st = ensure_smem_attr((const void*)potrf_rescue_kernel, kRSmemBytes, kSlotRescue)) return st;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)device_sms(), 1, 1);
@@ -249,7 +258,7 @@ int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   TraceScope ts(kKRescue, s);
-  e = cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, mode, gstate, bar, info);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, mode, gstate, bar, info);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_rescue_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }
