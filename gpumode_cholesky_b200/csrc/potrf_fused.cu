@@ -92,7 +92,8 @@ __device__ __forceinline__ void p_form(float (&p)[32], const float* A, int n, in
 template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info) {
+                       uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info,
+                       float2* __restrict__ piv) {
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
@@ -281,6 +282,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
             ok = false;
             break;
           }
+          // The pivot record of a guarded call: (L_jj, A_jj).
+          if (piv != nullptr && tid < 64)
+            piv[(size_t)b * n + k0 + tid] = make_float2(dg.S[tid * kD64Ld + tid], __ldg(A + (size_t)(k0 + tid) * (n + 1)));
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
           for (int e = tid; e < 64 * 16; e += kFThreads) {
@@ -342,7 +346,7 @@ bool fused_supported(int64_t n, int mode) {
 }
 
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s) {
+                int32_t* info, cudaStream_t s, float2* piv) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -355,10 +359,10 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
   if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
-    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
+    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, piv);
   } else {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
-    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info);
+    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, piv);
   }
   return check_launch("potrf_fused_kernel");
 }

@@ -5,8 +5,9 @@
 //   1. guard_audit_kernel audits every matrix's computed pivots L_jj^2
 //      against the mode's bound and writes the first failing block column
 //      per matrix, or -1, into the guard state (contiguous matrix ranges per
-//      CTA; one strided pass over the diagonals of A and L); it also resets
-//      the rescue's grid barrier;
+//      CTA; one coalesced pass over the (L_jj, A_jj) pairs the path
+//      recorded next to writing L_kk); it also resets the rescue's grid
+//      barrier;
 //   2. potrf_rescue_kernel reads the guard state and returns when no matrix
 //      failed (the usual case); otherwise it refactors every failing matrix
 //      from its first column in plain FP32 and overwrites its L and info;
@@ -44,7 +45,11 @@ constexpr uint32_t kRListOff = kRRowsOff + kRThreads * kRRowLd * 4;
 constexpr uint32_t kRMiscOff = kRListOff + kRList * 8;
 constexpr uint32_t kRSmemBytes = kRMiscOff + 64 + 128;
 
-size_t guard_ws_bytes(int64_t batch) { return (((size_t)batch * sizeof(int32_t) + 255) & ~(size_t)255) + 256; }
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+size_t guard_piv_offset(int64_t batch) { return align256((size_t)batch * sizeof(int32_t)); }
+size_t guard_ws_bytes(int64_t batch, int64_t n) {
+  return guard_piv_offset(batch) + align256((size_t)batch * (size_t)n * sizeof(float2)) + 256;
+}
 
 // Grid-wide barrier over the launch's CTAs: bar[0] counts arrivals, bar[1]
 // is the generation.  Bounded: false when the generation did not move.
@@ -82,11 +87,10 @@ __device__ __forceinline__ bool rescue_grid_sync(int* bar, int* s_ok) {
 // of each matrix is an atomic minimum in shared memory (in rounds of
 // 2 kRList matrices when the range is longer).
 __global__ void __launch_bounds__(kRThreads)
-    guard_audit_kernel(const float* __restrict__ a, const float* __restrict__ l, int64_t batch, int n, int mode,
-                       int32_t* __restrict__ gstate, int* bar) {
+    guard_audit_kernel(const float2* __restrict__ piv, int64_t batch, int n, int mode, int32_t* __restrict__ gstate,
+                       int* bar) {
   __shared__ int first[2 * kRList];
   const int tid = threadIdx.x;
-  const size_t n2 = (size_t)n * n;
   if (blockIdx.x == 0 && tid == 0) bar[0] = bar[1] = 0;  // the rescue's grid barrier
   {
     const int64_t per = (batch + gridDim.x - 1) / gridDim.x;
@@ -98,8 +102,7 @@ __global__ void __launch_bounds__(kRThreads)
       for (int i = tid; i < cnt; i += kRThreads) first[i] = 0x7fffffff;
       __syncthreads();
       // cnt <= 2 kRList and npiv < 2^16: the pair index fits 32 bits.  Eight
-      // pairs per thread are loaded before any is tested (latency-bound
-      // strided loads: one 32-byte sector each).
+      // pairs per thread are loaded before any is tested.
       const int total = cnt * npiv;
       for (int e0 = tid; e0 < total; e0 += 8 * kRThreads) {
         float lv[8], av[8];
@@ -112,9 +115,9 @@ __global__ void __launch_bounds__(kRThreads)
           lv[u] = 1.0f;
           av[u] = 0.0f;
           if (e < total) {
-            const size_t off = (size_t)(r0 + iv[u]) * n2 + (size_t)jv[u] * (n + 1);
-            lv[u] = __ldcg(l + off);
-            av[u] = __ldg(a + off);
+            const float2 pv = __ldcg(piv + (size_t)(r0 + iv[u]) * n + jv[u]);
+            lv[u] = pv.x;
+            av[u] = pv.y;
           }
         }
 #pragma unroll
@@ -238,12 +241,12 @@ __global__ void __launch_bounds__(kRThreads, 1)
   }
 }
 
-int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, int* bar, int32_t* info,
-                 cudaStream_t s) {
+int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, const float2* piv,
+                 int* bar, int32_t* info, cudaStream_t s) {
   if (batch == 0) return B2P_OK;
   {
     TraceScope ts(kKAudit, s);
-    guard_audit_kernel<<<(unsigned)device_sms(), kRThreads, 0, s>>>(a, l, batch, n, mode, gstate, bar);
+    guard_audit_kernel<<<(unsigned)device_sms(), kRThreads, 0, s>>>(piv, batch, n, mode, gstate, bar);
     if (int st = check_launch("guard_audit_kernel")) return st;
   }
   if (int st = ensure_smem_attr((const void*)potrf_rescue_kernel, kRSmemBytes, kSlotRescue)) return st;

@@ -510,7 +510,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 2)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info, const float* __restrict__ sig) {
+                      int32_t* __restrict__ info, const float* __restrict__ sig, float2* __restrict__ piv) {
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -644,6 +644,10 @@ __global__ void __launch_bounds__(kSThreads, 2)
             make_float4(c <= r ? srow[0] : 0.f, c + 1 <= r ? srow[1] : 0.f, c + 2 <= r ? srow[2] : 0.f,
                         c + 3 <= r ? srow[3] : 0.f);
       }
+      // The pivot record of a guarded call: (L_jj, A_jj).
+      if (piv != nullptr && tid < 64)
+        piv[(size_t)b * n + k0 + tid] =
+            make_float2(dg.S[tid * kD64Ld + tid], __ldg(a + (size_t)b * n2 + (size_t)(k0 + tid) * (n + 1)));
       if (tid == 0 && info != nullptr) {
         if (bad == kDiagTimeout)
           info[b] = -1;
@@ -826,7 +830,7 @@ int side_stream(SideStream** out) {
 // wide kernel keeps to a bounded number of SMs so that the steps, which
 // carry the critical path, always find free ones.
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s) {
+                int32_t* info, cudaStream_t s, float2* piv) {
   const size_t need = split_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -973,7 +977,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       TraceScope ts(kKSplitStep, s,
                     batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
       const cudaError_t e =
-          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, (const float*)sig);
+          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, (const float*)sig, piv);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,
