@@ -103,11 +103,11 @@ size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode) {
 }
 
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
-               int32_t* info, cudaStream_t s, float2* piv) {
+               int32_t* info, cudaStream_t s, GuardRec grd) {
   switch (path) {
-    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s, piv);
-    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s, piv);
-    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s, piv);
+    case B2P_PATH_FUSED: return potrf_fused(a, l, batch, n, mode, ws, ws_bytes, info, s, grd);
+    case B2P_PATH_FUSED_WS: return potrf_fused_ws(a, l, batch, n, mode, ws, ws_bytes, info, s, grd);
+    case B2P_PATH_SPLIT: return potrf_split(a, l, batch, n, mode, ws, ws_bytes, info, s, grd);
     default: return potrf_blocked(a, l, batch, n, mode, ws, ws_bytes, info, s);
   }
 }
@@ -190,16 +190,14 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
   // The guarded paths' state (first failing block column per matrix, -1
   // for none: the caller's fp32_from when given) and the rescue's barrier
   // words sit ahead of the path's own workspace.
-  int32_t* gstate = nullptr;
-  float2* gpiv = nullptr;
-  int* gbar = nullptr;
+  GuardRec grd;
   if (guard) {
     const size_t gb = guard_ws_bytes(batch, n);
     if (workspace == nullptr || workspace_bytes < gb)
       return set_error(B2P_ERR_WORKSPACE, "workspace of at least %zu bytes required, %zu given", gb, workspace_bytes);
-    gstate = fp32_from ? fp32_from : static_cast<int32_t*>(workspace);
-    gpiv = reinterpret_cast<float2*>(static_cast<uint8_t*>(workspace) + guard_piv_offset(batch));
-    gbar = reinterpret_cast<int*>(static_cast<uint8_t*>(workspace) + gb - 256);
+    grd.state = fp32_from ? fp32_from : static_cast<int32_t*>(workspace);
+    grd.piv = reinterpret_cast<float2*>(static_cast<uint8_t*>(workspace) + guard_piv_offset(batch));
+    grd.bar = reinterpret_cast<int*>(static_cast<uint8_t*>(workspace) + gb - 256);
     workspace = static_cast<uint8_t*>(workspace) + gb;
     workspace_bytes -= gb;
   }
@@ -222,21 +220,22 @@ int b2p_potrf_batched_ex(const float* a, float* l, int64_t batch, int64_t n, int
     const int64_t tail = batch % per;
     if (batch > per && tail > 0 && tail * 2 <= per && fused_ws_supported(tail, n, mode)) {
       const int64_t head = batch - tail;
-      st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, gpiv);
+      st = potrf_fused(a, l, head, (int)n, mode, workspace, workspace_bytes, info, s, grd);
       if (st == B2P_OK) {
         const size_t moff = (size_t)head * (size_t)n * (size_t)n;
         const size_t woff = (size_t)head * 2 * panel_copy_region_bytes((int)n);
         st = potrf_fused_ws(a + moff, l + moff, tail, (int)n, mode, static_cast<uint8_t*>(workspace) + woff,
                             workspace_bytes - woff, info ? info + head : nullptr, s,
-                            gpiv ? gpiv + (size_t)head * (size_t)n : nullptr);
+                            guard ? GuardRec{grd.piv + (size_t)head * (size_t)n, grd.state + head, grd.bar}
+                                  : GuardRec());
       }
       done = true;
     }
   }
-  if (!done) st = potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, gpiv);
+  if (!done) st = potrf_path(a, l, batch, (int)n, mode, path, workspace, workspace_bytes, info, s, grd);
   if (st != B2P_OK || !guard) return st;
-  // Audit the pivots and refactor in FP32 every matrix whose pivots fail.
-  return guard_rescue(a, l, batch, (int)n, mode, gstate, gpiv, gbar, info, s);
+  // Refactor in FP32 every matrix whose pivots failed the path's audit.
+  return guard_rescue(a, l, batch, (int)n, mode, grd, info, s);
 }
 
 size_t b2p_potrf_backward_workspace_size(int64_t batch, int64_t n) {

@@ -57,6 +57,28 @@ __device__ __forceinline__ float guard_tau(int mode, int k) {
   return kGuardMargin * (rep + steps * (float)k * 1.1920928955078125e-7f);  // 2^-23 per step
 }
 
+// The audit of one finished matrix: the first block column whose recorded
+// pivot (L_jj, A_jj) fails L_jj^2 > guard_tau * A_jj (or is not finite), or
+// -1.  piv is the matrix's record (n pairs; column 0 has no update and is
+// not tested), written earlier by threads of this CTA or by earlier
+// launches.  Collective over the NT threads that call it (barrier functor
+// `bar`); smin is one int of shared memory, free until the call returns.
+template <int NT, class Bar>
+__device__ __forceinline__ int guard_audit_matrix(const float2* piv, int n, int mode, int* smin, int tid, Bar bar) {
+  if (tid == 0) *smin = 0x7fffffff;
+  bar();
+  int first = 0x7fffffff;
+  for (int j = 64 + tid; j < n; j += NT) {
+    const float2 p = __ldcg(piv + j);
+    if (!(p.x * p.x > guard_tau(mode, j >> 6) * p.y)) first = min(first, j >> 6);
+  }
+  if (first != 0x7fffffff) atomicMin(smin, first);
+  bar();
+  const int f = *smin;
+  bar();
+  return f == 0x7fffffff ? -1 : f;
+}
+
 // FP32 update of one row against 32 columns of block column k, computed on
 // the SIMT cores: d[q] = sum_{j < k0} L[row][j] * L[k0 + c0 + q][j], each
 // 32-wide piece of j summed on its own (fused multiply-adds in order of j)

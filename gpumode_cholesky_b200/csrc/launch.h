@@ -40,14 +40,22 @@ int ragged_blocked_step(const float* a, float* l, const RaggedTables& t, const R
 // Fused left-looking tensor-core path for 128 < n <= 1024, n % 64 == 0 (potrf_fused.cu).
 bool fused_supported(int64_t n, int mode);
 size_t fused_workspace_bytes(int64_t batch, int64_t n);
-// piv (guarded calls, else nullptr): every matrix's pivots as (L_jj, A_jj),
-// batch x n float2, for the pivot guard's audit.
+// The pivot guard's device state for one guarded call (all null otherwise):
+// the pivot record, (L_jj, A_jj) per pivot (batch x n), written next to L_kk;
+// the first failing block column per matrix (-1 for none), which the path
+// writes when it finishes a matrix (the audit); the rescue's two grid-barrier
+// words, which the path resets.
+struct GuardRec {
+  float2* piv = nullptr;
+  int32_t* state = nullptr;
+  int* bar = nullptr;
+};
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, float2* piv = nullptr);
+                int32_t* info, cudaStream_t s, GuardRec grd = GuardRec());
 // Warp-specialized variant (potrf_fused_ws.cu), in clusters of up to 8 CTAs
 // per matrix for small batches: same workspace and contract.
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                   int32_t* info, cudaStream_t s, float2* piv = nullptr);
+                   int32_t* info, cudaStream_t s, GuardRec grd = GuardRec());
 // Orders and batches the warp-specialized kernel can take (n <= 8192, in
 // clusters large enough for TMEM), and the subset the dispatcher and the
 // forced-path entry point offer (n <= 1024).
@@ -57,21 +65,21 @@ bool fused_ws_supported(int64_t batch, int64_t n, int mode);
 // Pivot guard (guard.cuh, potrf_rescue.cu).  A guarded call keeps, ahead of
 // its path's own workspace, guard_ws_bytes(batch, n): the per-matrix guard
 // state (int32: first failing block column, -1 for none; the caller's
-// fp32_from array takes its place when given), the pivot record the path
-// writes (guard_piv_offset: (L_jj, A_jj) per pivot) and two barrier words.
-// guard_rescue audits the recorded pivots of the tensor-mode path (mode) and
-// refactors in FP32 every matrix whose pivots fail.
+// fp32_from array takes its place when given), the pivot record
+// (guard_piv_offset) and two barrier words, all filled by the path's
+// kernels (GuardRec).  guard_rescue then refactors in FP32 every matrix
+// whose pivots failed.
 size_t guard_ws_bytes(int64_t batch, int64_t n);
 size_t guard_piv_offset(int64_t batch);
-int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, const float2* piv,
-                 int* bar, int32_t* info, cudaStream_t s);
+int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, const GuardRec& grd, int32_t* info,
+                 cudaStream_t s);
 
 // Multi-CTA left-looking tensor-core path (potrf_split.cu): n % 64 == 0,
 // n > 128, tensor modes; two launches per 64-wide block column.
 bool split_supported(int64_t n, int mode);
 size_t split_workspace_bytes(int64_t batch, int64_t n);
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, float2* piv = nullptr);
+                int32_t* info, cudaStream_t s, GuardRec grd = GuardRec());
 
 // The n > 128 dispatcher (capi.cu): the path for (batch, n, mode), whether a
 // path takes a shape, its workspace, and a launch on an explicit path (n > 128;
@@ -80,7 +88,7 @@ int choose_path(int64_t batch, int64_t n, int mode);
 bool path_supported(int path, int64_t batch, int64_t n, int mode);
 size_t path_workspace_bytes(int path, int64_t batch, int64_t n, int mode);
 int potrf_path(const float* a, float* l, int64_t batch, int n, int mode, int path, void* ws, size_t ws_bytes,
-               int32_t* info, cudaStream_t s, float2* piv = nullptr);
+               int32_t* info, cudaStream_t s, GuardRec grd = GuardRec());
 
 // Batched triangular solves with L (trsv.cu): x = L^{-1} b, or L^{-T} b.
 constexpr int kTrsvMaxN = 32768;  // x is held in shared memory (n floats)
@@ -145,7 +153,6 @@ enum KernelId {
   kKGpForward,
   kKGpLbar,
   kKRescue,
-  kKAudit,
   kKCount
 };
 

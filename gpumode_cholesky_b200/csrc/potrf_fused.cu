@@ -29,6 +29,7 @@
 #include <algorithm>
 
 #include "diag64.cuh"
+#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -93,7 +94,10 @@ template <int MODE>
 __global__ void __launch_bounds__(kFThreads, 2)
     potrf_fused_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
                        uint8_t* __restrict__ ws, uint32_t tmem_cols, int32_t* __restrict__ info,
-                       float2* __restrict__ piv) {
+                       GuardRec grd) {
+  __shared__ int s_gmin;
+  // The rescue's grid barrier starts from zero (it runs after this kernel).
+  if (grd.bar != nullptr && blockIdx.x == 0 && threadIdx.x == 0) grd.bar[0] = grd.bar[1] = 0;
   extern __shared__ unsigned char fraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(fraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm);
@@ -283,8 +287,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
             break;
           }
           // The pivot record of a guarded call: (L_jj, A_jj).
-          if (piv != nullptr && tid < 64)
-            piv[(size_t)b * n + k0 + tid] = make_float2(dg.S[tid * kD64Ld + tid], __ldg(A + (size_t)(k0 + tid) * (n + 1)));
+          if (grd.piv != nullptr && tid < 64)
+            grd.piv[(size_t)b * n + k0 + tid] =
+                make_float2(dg.S[tid * kD64Ld + tid], __ldg(A + (size_t)(k0 + tid) * (n + 1)));
           if (tid == 0 && bad >= 0 && *badp < 0) *badp = k0 + bad;
           // L_kk (zeros above its diagonal), row-major, float4.
           for (int e = tid; e < 64 * 16; e += kFThreads) {
@@ -322,7 +327,15 @@ __global__ void __launch_bounds__(kFThreads, 2)
       umma::fence_after_sync();
     }
     if (tid == 0 && info != nullptr) info[b] = ok ? (*badp < 0 ? 0 : *badp + 1) : -1;
+    if (grd.state != nullptr) {
+      const int f = ok ? guard_audit_matrix<kFThreads>(grd.piv + (size_t)b * n, n, MODE, &s_gmin, tid, CtaBarrier())
+                       : -1;
+      if (tid == 0) grd.state[b] = f;
+    }
   }
+  // Matrices this CTA did not reach (a bounded wait gave up) are not rescued.
+  if (grd.state != nullptr && tid == 0)
+    for (; b < batch; b += gridDim.x) grd.state[b] = -1;
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == kFStripThread) umma::bulk_wait_all();
   // Release TMEM after a last bounded chance for outstanding MMAs.
@@ -346,7 +359,7 @@ bool fused_supported(int64_t n, int mode) {
 }
 
 int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, float2* piv) {
+                int32_t* info, cudaStream_t s, GuardRec grd) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -359,10 +372,10 @@ int potrf_fused(const float* a, float* l, int64_t batch, int n, int mode, void* 
   TraceScope ts(kKFused, s, (double)batch * n * n * n / 3.0);
   if ((mode & B2P_MODE_MASK) == B2P_MODE_TF32) {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_TF32>, smem, kSlotFused0)) return st;
-    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, piv);
+    potrf_fused_kernel<B2P_MODE_TF32><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, grd);
   } else {
     if (int st = ensure_smem_attr((const void*)potrf_fused_kernel<B2P_MODE_BF16X3>, smem, kSlotFused1)) return st;
-    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, piv);
+    potrf_fused_kernel<B2P_MODE_BF16X3><<<grid, kFThreads, smem, s>>>(a, l, batch, n, wsa, cols, info, grd);
   }
   return check_launch("potrf_fused_kernel");
 }

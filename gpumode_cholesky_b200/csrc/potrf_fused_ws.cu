@@ -40,6 +40,7 @@
 #include <algorithm>
 
 #include "diag64.cuh"
+#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -238,7 +239,8 @@ __device__ void ws_producer(const WsBars& br, uint8_t* sm, uint8_t* ws, int64_t 
 // Consumers: warps 0-7.
 template <int MODE, int CL>
 __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, float* l, uint8_t* ws, int64_t batch,
-                             int n, uint32_t tmem, int32_t* info, int rank, float2* piv) {
+                             int n, uint32_t tmem, int32_t* info, int rank, GuardRec grd) {
+  __shared__ int s_gmin;
   const ConsumerBar cbar;
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kWDiagOff);
   float* PtT = reinterpret_cast<float*>(sm + kWPtOff);
@@ -389,8 +391,9 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
           }
           if (tid == 0 && bad >= 0 && *br.badp < 0) *br.badp = k0 + bad;
           // The pivot record of a guarded call: (L_jj, A_jj).
-          if (piv != nullptr && rank == 0 && tid < 64)
-            piv[(size_t)b * n + k0 + tid] = make_float2(dg.S[tid * kD64Ld + tid], __ldg(A + (size_t)(k0 + tid) * (n + 1)));
+          if (grd.piv != nullptr && rank == 0 && tid < 64)
+            grd.piv[(size_t)b * n + k0 + tid] =
+                make_float2(dg.S[tid * kD64Ld + tid], __ldg(A + (size_t)(k0 + tid) * (n + 1)));
           for (int e = tid; e < (rank == 0 ? 64 * 16 : 0); e += kWConsumers) {
             const int r = e >> 4, c = (e & 15) * 4;
             const float* srow = dg.S + r * kD64Ld + c;
@@ -435,7 +438,17 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
       }
     }
     if (tid == 0 && rank == 0 && info != nullptr) info[b] = failed ? -1 : (*br.badp < 0 ? 0 : *br.badp + 1);
-    if (failed) break;
+    if (grd.state != nullptr && rank == 0) {
+      const int f =
+          failed ? -1 : guard_audit_matrix<kWConsumers>(grd.piv + (size_t)b * n, n, MODE, &s_gmin, tid, cbar);
+      if (tid == 0) grd.state[b] = f;
+    }
+    if (failed) {
+      // Matrices this cluster did not reach are not rescued.
+      if (grd.state != nullptr && rank == 0 && tid == 0)
+        for (int64_t b2 = b + gridDim.x / CL; b2 < batch; b2 += gridDim.x / CL) grd.state[b2] = -1;
+      break;
+    }
   }
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == kWStripThread) umma::bulk_wait_all();
@@ -444,7 +457,9 @@ __device__ void ws_consumers(const WsBars& br, uint8_t* sm, const float* a, floa
 template <int MODE, int CL>
 __global__ void __launch_bounds__(kWThreads, 1)
     potrf_fused_ws_kernel(const float* __restrict__ a, float* __restrict__ l, int64_t batch, int n,
-                          uint8_t* __restrict__ ws, int32_t* __restrict__ info, float2* __restrict__ piv) {
+                          uint8_t* __restrict__ ws, int32_t* __restrict__ info, GuardRec grd) {
+  // The rescue's grid barrier starts from zero (it runs after this kernel).
+  if (grd.bar != nullptr && blockIdx.x == 0 && threadIdx.x == 0) grd.bar[0] = grd.bar[1] = 0;
   extern __shared__ unsigned char wraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(wraw) + 1023) & ~(uintptr_t)1023);
   WsBars br;
@@ -486,7 +501,7 @@ __global__ void __launch_bounds__(kWThreads, 1)
   if (warp == kWConsumers / 32) {
     if ((tid & 31) == 0) ws_producer<MODE, CL>(br, sm, ws, batch, n, tmem, rank);
   } else {
-    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank, piv);
+    ws_consumers<MODE, CL>(br, sm, a, l, ws, batch, n, tmem, info, rank, grd);
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -523,7 +538,7 @@ bool fused_ws_fits(int64_t batch, int64_t n, int mode) {
 bool fused_ws_supported(int64_t batch, int64_t n, int mode) { return n <= 1024 && fused_ws_fits(batch, n, mode); }
 
 int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                   int32_t* info, cudaStream_t s, float2* piv) {
+                   int32_t* info, cudaStream_t s, GuardRec grd) {
   const size_t need = fused_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -534,7 +549,7 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
     return set_error(B2P_ERR_UNSUPPORTED, "warp-specialized path: n=%d not supported", n);
   const int grid = cl * (int)std::max<int64_t>(1, std::min<int64_t>(batch, sms / cl));
   const bool tf32 = (mode & B2P_MODE_MASK) == B2P_MODE_TF32;
-  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*, float2*);
+  using Kern = void (*)(const float*, float*, int64_t, int, uint8_t*, int32_t*, GuardRec);
   static const Kern kernels[2][4] = {
       {potrf_fused_ws_kernel<B2P_MODE_TF32, 1>, potrf_fused_ws_kernel<B2P_MODE_TF32, 2>,
        potrf_fused_ws_kernel<B2P_MODE_TF32, 4>, potrf_fused_ws_kernel<B2P_MODE_TF32, 8>},
@@ -556,7 +571,7 @@ int potrf_fused_ws(const float* a, float* l, int64_t batch, int n, int mode, voi
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   TraceScope ts(kKFusedWs, s, (double)batch * n * n * n / 3.0);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, piv);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, a, l, batch, n, wsa, info, grd);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_fused_ws_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }

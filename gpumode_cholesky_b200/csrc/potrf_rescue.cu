@@ -1,19 +1,13 @@
 // Pivot audit and FP32 rescue of the pivot guard (guard.cuh).
 //
-// Right after a tensor-mode path (potrf_fused.cu, potrf_fused_ws.cu,
-// potrf_split.cu) has factored a batch, on the same stream, two launches:
-//   1. guard_audit_kernel audits every matrix's computed pivots L_jj^2
-//      against the mode's bound and writes the first failing block column
-//      per matrix, or -1, into the guard state (contiguous matrix ranges per
-//      CTA; one coalesced pass over the (L_jj, A_jj) pairs the path
-//      recorded next to writing L_kk); it also resets the rescue's grid
-//      barrier;
-//   2. potrf_rescue_kernel reads the guard state and returns when no matrix
-//      failed (the usual case); otherwise it refactors every failing matrix
-//      from its first column in plain FP32 and overwrites its L and info;
-//      the others are not touched.
-// The kernel boundary between them is the audit's grid-wide barrier, so the
-// usual case waits on no spin.
+// The tensor-mode paths (potrf_fused.cu, potrf_fused_ws.cu, potrf_split.cu)
+// audit each matrix when they finish it (guard_audit_matrix over the
+// (L_jj, A_jj) pairs they recorded next to writing L_kk), write its guard
+// state (the first failing block column, or -1) and reset this kernel's grid
+// barrier.  Right after, on the same stream, potrf_rescue_kernel reads the
+// guard state and returns when no matrix failed (the usual case, one short
+// launch); otherwise it refactors every failing matrix from its first column
+// in plain FP32 and overwrites its L and info; the others are not touched.
 //
 // Rescue schedule: one cooperative launch, one CTA per SM (all CTAs
 // resident at once), left-looking by 64-wide block columns.  In column k the jobs are
@@ -79,56 +73,6 @@ __device__ __forceinline__ bool rescue_grid_sync(int* bar, int* s_ok) {
   }
   __syncthreads();
   return *s_ok != 0;
-}
-
-// The audit (step 1 above): the first block column whose pivot fails, per
-// matrix.  Each CTA takes a contiguous range of matrices, its threads stride
-// over all their (matrix, pivot) pairs at once, and the first failing column
-// of each matrix is an atomic minimum in shared memory (in rounds of
-// 2 kRList matrices when the range is longer).
-__global__ void __launch_bounds__(kRThreads)
-    guard_audit_kernel(const float2* __restrict__ piv, int64_t batch, int n, int mode, int32_t* __restrict__ gstate,
-                       int* bar) {
-  __shared__ int first[2 * kRList];
-  const int tid = threadIdx.x;
-  if (blockIdx.x == 0 && tid == 0) bar[0] = bar[1] = 0;  // the rescue's grid barrier
-  {
-    const int64_t per = (batch + gridDim.x - 1) / gridDim.x;
-    const int64_t lo0 = per * (int64_t)blockIdx.x;
-    const int64_t lo = lo0 < batch ? lo0 : batch, hi = lo + per < batch ? lo + per : batch;
-    const int npiv = n - 64;  // pivots 64 .. n-1 (block column 0 has no update)
-    for (int64_t r0 = lo; r0 < hi; r0 += 2 * kRList) {
-      const int cnt = (int)(hi - r0 < 2 * kRList ? hi - r0 : 2 * kRList);
-      for (int i = tid; i < cnt; i += kRThreads) first[i] = 0x7fffffff;
-      __syncthreads();
-      // cnt <= 2 kRList and npiv < 2^16: the pair index fits 32 bits.  Eight
-      // pairs per thread are loaded before any is tested.
-      const int total = cnt * npiv;
-      for (int e0 = tid; e0 < total; e0 += 8 * kRThreads) {
-        float lv[8], av[8];
-        int iv[8], jv[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int e = e0 + u * kRThreads;
-          iv[u] = e / npiv;
-          jv[u] = 64 + (e - iv[u] * npiv);
-          lv[u] = 1.0f;
-          av[u] = 0.0f;
-          if (e < total) {
-            const float2 pv = __ldcg(piv + (size_t)(r0 + iv[u]) * n + jv[u]);
-            lv[u] = pv.x;
-            av[u] = pv.y;
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (!(lv[u] * lv[u] > guard_tau(mode, jv[u] >> 6) * av[u])) atomicMin(first + iv[u], jv[u] >> 6);
-      }
-      __syncthreads();
-      for (int i = tid; i < cnt; i += kRThreads) gstate[r0 + i] = first[i] == 0x7fffffff ? -1 : first[i];
-      __syncthreads();
-    }
-  }
 }
 
 __global__ void __launch_bounds__(kRThreads, 1)
@@ -241,14 +185,9 @@ __global__ void __launch_bounds__(kRThreads, 1)
   }
 }
 
-int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32_t* gstate, const float2* piv,
-                 int* bar, int32_t* info, cudaStream_t s) {
+int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, const GuardRec& grd, int32_t* info,
+                 cudaStream_t s) {
   if (batch == 0) return B2P_OK;
-  {
-    TraceScope ts(kKAudit, s);
-    guard_audit_kernel<<<(unsigned)device_sms(), kRThreads, 0, s>>>(piv, batch, n, mode, gstate, bar);
-    if (int st = check_launch("guard_audit_kernel")) return st;
-  }
   if (int st = ensure_smem_attr((const void*)potrf_rescue_kernel, kRSmemBytes, kSlotRescue)) return st;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)device_sms(), 1, 1);
@@ -261,7 +200,8 @@ int guard_rescue(const float* a, float* l, int64_t batch, int n, int mode, int32
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   TraceScope ts(kKRescue, s);
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, mode, gstate, bar, info);
+  const cudaError_t e =
+      cudaLaunchKernelEx(&cfg, potrf_rescue_kernel, a, l, batch, n, mode, grd.state, grd.bar, info);
   if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "potrf_rescue_kernel: %s", cudaGetErrorString(e));
   return B2P_OK;
 }

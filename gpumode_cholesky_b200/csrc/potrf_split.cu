@@ -45,6 +45,7 @@
 #include <mutex>
 
 #include "diag64.cuh"
+#include "guard.cuh"
 #include "launch.h"
 #include "panel_copy.cuh"
 #include "umma.cuh"
@@ -510,7 +511,10 @@ template <int MODE>
 __global__ void __launch_bounds__(kSThreads, 2)
     split_step_kernel(const float* __restrict__ a, float* __restrict__ l, uint8_t* __restrict__ ws,
                       const float* __restrict__ pbuf, int64_t batch, int n, int k, int G,
-                      int32_t* __restrict__ info, const float* __restrict__ sig, float2* __restrict__ piv) {
+                      int32_t* __restrict__ info, const float* __restrict__ sig, GuardRec grd) {
+  __shared__ int s_gmin;
+  // The last step resets the rescue's grid barrier (the rescue runs after it).
+  if (grd.bar != nullptr && k == n / 64 - 1 && blockIdx.x == 0 && threadIdx.x == 0) grd.bar[0] = grd.bar[1] = 0;
   extern __shared__ unsigned char sraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(sraw) + 1023) & ~(uintptr_t)1023);
   Diag64Smem& dg = *reinterpret_cast<Diag64Smem*>(sm + kSDiag);
@@ -545,7 +549,8 @@ __global__ void __launch_bounds__(kSThreads, 2)
   uint32_t ph_full = 0u, ph_done = 0u;
   bool ok = true;
 
-  for (int64_t job = blockIdx.x; job < batch * G && ok; job += gridDim.x) {
+  int64_t job = blockIdx.x;
+  for (; job < batch * G && ok; job += gridDim.x) {
     const int64_t b = job / G;
     const int g = (int)(job - b * G);
     float* L = l + (size_t)b * n2;
@@ -644,10 +649,15 @@ __global__ void __launch_bounds__(kSThreads, 2)
             make_float4(c <= r ? srow[0] : 0.f, c + 1 <= r ? srow[1] : 0.f, c + 2 <= r ? srow[2] : 0.f,
                         c + 3 <= r ? srow[3] : 0.f);
       }
-      // The pivot record of a guarded call: (L_jj, A_jj).
-      if (piv != nullptr && tid < 64)
-        piv[(size_t)b * n + k0 + tid] =
+      // The pivot record of a guarded call: (L_jj, A_jj); after the last
+      // block column, the matrix's audit.
+      if (grd.piv != nullptr && tid < 64)
+        grd.piv[(size_t)b * n + k0 + tid] =
             make_float2(dg.S[tid * kD64Ld + tid], __ldg(a + (size_t)b * n2 + (size_t)(k0 + tid) * (n + 1)));
+      if (grd.state != nullptr && k == N - 1) {
+        const int f = guard_audit_matrix<kSThreads>(grd.piv + (size_t)b * n, n, MODE, &s_gmin, tid, CtaBarrier());
+        if (tid == 0) grd.state[b] = f;
+      }
       if (tid == 0 && info != nullptr) {
         if (bad == kDiagTimeout)
           info[b] = -1;
@@ -713,6 +723,10 @@ __global__ void __launch_bounds__(kSThreads, 2)
     // dg is rewritten by the next job.
     __syncthreads();
   }
+  // Matrices whose last step this CTA did not reach are not rescued.
+  if (!ok && grd.state != nullptr && k == N - 1 && tid == 0)
+    for (; job < batch * G; job += gridDim.x)
+      if (job % G == 0) grd.state[job / G] = -1;
   if (!ok) umma::mbar_wait_bounded(done, ph_done, kSplitPolls);
   // The strip's bulk stores read the zero buffer until they complete.
   if (tid == kSStripThread) umma::bulk_wait_all();
@@ -830,7 +844,7 @@ int side_stream(SideStream** out) {
 // wide kernel keeps to a bounded number of SMs so that the steps, which
 // carry the critical path, always find free ones.
 int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* ws, size_t ws_bytes,
-                int32_t* info, cudaStream_t s, float2* piv) {
+                int32_t* info, cudaStream_t s, GuardRec grd) {
   const size_t need = split_workspace_bytes(batch, n);
   if (ws == nullptr || ws_bytes < need)
     return set_error(B2P_ERR_WORKSPACE, "workspace of %zu bytes required, %zu given", need, ws_bytes);
@@ -977,7 +991,7 @@ int potrf_split(const float* a, float* l, int64_t batch, int n, int mode, void* 
       TraceScope ts(kKSplitStep, s,
                     batch * (64.0 * 64 * 64 / 3 + rows * 64 * 64 + (k > 0 ? 2.0 * 64 * 64 * (rows + 64) : 0.0)));
       const cudaError_t e =
-          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, (const float*)sig, piv);
+          cudaLaunchKernelEx(&cfg, stp, a, l, copies, (const float*)pk, batch, n, k, G, info, (const float*)sig, grd);
       if (e != cudaSuccess) return set_error(B2P_ERR_CUDA, "split_step_kernel: %s", cudaGetErrorString(e));
     }
     // Outer block J = (k + 1) / W + 1 needs the panels before block J - 1,

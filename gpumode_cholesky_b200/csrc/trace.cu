@@ -22,7 +22,7 @@ const char* const kNames[kKCount] = {
     "panel_kernel",        "trail_kernel",        "trail_tc_kernel",   "split_step_kernel",
     "split_update_kernel", "ragged_gather_kernel", "bwd_gemm_kernel",   "bwd_trsm_kernel",
     "bwd_sym_kernel",      "potrf_fused_kernel",  "potrf_fused_ws_kernel", "ragged_scatter_kernel", "split_wide_kernel",
-    "trsv_kernel",         "gp_forward_kernel",   "gp_lbar_kernel",       "potrf_rescue_kernel", "guard_audit_kernel"};
+    "trsv_kernel",         "gp_forward_kernel",   "gp_lbar_kernel",       "potrf_rescue_kernel"};
 
 void free_all() {
   for (auto& e : g_entries) {
