@@ -249,40 +249,43 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     const int kmax = 8 * ti > 4 * tj ? 8 * ti : 4 * tj;  // smallest max(i, j) of the tile
     if (lower) bs_tile(bA, bB, ti, tj, kmax, 128, acc);
     __syncthreads();
-    // P^T into bB.
+    // P^T into bB: per column j of the tile, its 8 rows as two float4.
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
+    for (int c = 0; c < 4; ++c) {
+      const int j = 4 * tj + c;
+      float v[8];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 8 * ti + r, j = 4 * tj + c;
-        const float v = !lower || j > i ? 0.0f : (j == i ? 0.5f * acc[r][c] : acc[r][c]);
-        bB[j * kBsLd + i] = v;
+      for (int r = 0; r < 8; ++r) {
+        const int i = 8 * ti + r;
+        v[r] = !lower || j > i ? 0.0f : (j == i ? 0.5f * acc[r][c] : acc[r][c]);
       }
+      float4* dst = reinterpret_cast<float4*>(bB + j * kBsLd + 8 * ti);
+      dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+      dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
     // U = L^{-1} into bC.
     trtri128(bA, bC, kBsLd, sc.invd, work);
     // Z = P U: Z[i][j] = sum_k P^T[k][i] U[k][j], k in [j, i] (lower tiles).
     if (lower) bs_tile(bB, bC, ti, tj, 4 * tj, 8 * ti + 8, acc);
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int i = 8 * ti + r, j = 4 * tj + c;
-        bB[i * kBsLd + j] = (lower && j <= i) ? acc[r][c] : 0.0f;
-      }
+    for (int r = 0; r < 8; ++r) {
+      const int i = 8 * ti + r, j = 4 * tj;
+      *reinterpret_cast<float4*>(bB + i * kBsLd + j) =
+          make_float4((lower && j <= i) ? acc[r][0] : 0.0f, (lower && j + 1 <= i) ? acc[r][1] : 0.0f,
+                      (lower && j + 2 <= i) ? acc[r][2] : 0.0f, (lower && j + 3 <= i) ? acc[r][3] : 0.0f);
+    }
     __syncthreads();
     // S = U^T Z: S[i][j] = sum_k U[k][i] Z[k][j], k >= max(i, j); into bA.
     bs_tile(bC, bB, ti, tj, kmax, 128, acc);
 #pragma unroll
     for (int r = 0; r < 8; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) bA[(8 * ti + r) * kBsLd + 4 * tj + c] = acc[r][c];
+      *reinterpret_cast<float4*>(bA + (8 * ti + r) * kBsLd + 4 * tj) =
+          make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
     __syncthreads();
     float* Ab = abar + (size_t)b * n * n;
-    for (int e = tid; e < n * n; e += kBsThreads) {
-      const int i = e / n, j = e - (e / n) * n;
-      Ab[e] = 0.5f * (bA[i * kBsLd + j] + bA[j * kBsLd + i]);
-    }
+    for (int i = tid >> 5; i < n; i += kBsThreads / 32)
+      for (int j = tid & 31; j < n; j += 32) Ab[(size_t)i * n + j] = 0.5f * (bA[i * kBsLd + j] + bA[j * kBsLd + i]);
     __syncthreads();
   }
 }

@@ -39,11 +39,11 @@ __device__ __forceinline__ float ld_cluster_f32(const float* local, uint32_t ran
   return v;
 }
 
-// Solves the diagonal block at rows r0 .. r0 + m - 1 in place in x (one warp).
+// This lane's 32 values of the diagonal block at rows r0 .. r0 + m - 1: row
+// `lane` of it, or column `lane` for L^T (zeros outside its lower triangle).
 template <bool TRANS>
-__device__ __forceinline__ void solve_diag_block(const float* __restrict__ L, int n, int r0, int m, float* x) {
+__device__ __forceinline__ void load_diag_block(const float* __restrict__ L, int n, int r0, int m, float (&e)[32]) {
   const int lane = threadIdx.x & 31;
-  float e[32];  // TRANS: column `lane` of the block (e[j] = L[r0+j][r0+lane]); else row `lane`
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     float v = 0.0f;
@@ -54,6 +54,13 @@ __device__ __forceinline__ void solve_diag_block(const float* __restrict__ L, in
     }
     e[j] = v;
   }
+}
+
+// Solves the diagonal block at rows r0 .. r0 + m - 1 in place in x (one
+// warp), with e from load_diag_block.
+template <bool TRANS>
+__device__ __forceinline__ void solve_diag_block(const float (&e)[32], int r0, int m, float* x) {
+  const int lane = threadIdx.x & 31;
   float r = lane < m ? x[r0 + lane] : 0.0f;
   float inv = 0.0f;  // 1 / L_ii of this lane's row (e[lane] is the diagonal)
 #pragma unroll
@@ -122,7 +129,9 @@ __device__ void cluster_trsv(const float* __restrict__ L, int n, float* x, TrsvS
     const int r0 = 32 * blk, m = min(32, n - r0);
     const int owner = blk % C;
     if (rank == owner && tid < 32) {
-      solve_diag_block<TRANS>(L, n, r0, m, x);
+      float e[32];
+      load_diag_block<TRANS>(L, n, r0, m, e);
+      solve_diag_block<TRANS>(e, r0, m, x);
       if (tid < m) sh.bcast[s & 1][tid] = x[r0 + tid];
     }
     // The slot written at block s is rewritten at s + 2, after every CTA
@@ -190,6 +199,157 @@ __device__ void cluster_trsv(const float* __restrict__ L, int n, float* x, TrsvS
   }
 }
 
+// The same solve for n % 4 == 0 with the loads of L issued one step ahead:
+// the next step's diagonal block (by its owner's warp 0) while this step's
+// update runs, and this thread's first operands of the next update right
+// after this one, so that a step's critical path is the diagonal block's
+// shuffles, the barriers and the FMAs rather than two round trips to
+// memory.  Same barriers in the same order as cluster_trsv.  The update of
+// L^T runs as (column group of 4, group of 4 of the block's 32 rows) tasks,
+// eight per column group in consecutive lanes, summed by shuffles.
+template <bool TRANS>
+__device__ void cluster_trsv_ahead(const float* __restrict__ L, int n, float* x, TrsvShared& sh, int C, int rank) {
+  const int tid = threadIdx.x;
+  const int nb = (n + 31) / 32;
+  float e[32];         // the diagonal block of the current step (its owner's warp 0)
+  float v[32];         // L: this thread's first row of the update
+  float4 w[2][4];      // L^T: this thread's first two tasks of the update
+  // Own rows below block blk (L): 32 nown rows from own block `first` on.
+  auto rows_below = [&](int blk, int& first) {
+    first = blk + 1 + ((rank - (blk + 1) % C) % C + C) % C;
+    return first < nb ? 32 * ((nb - 1 - first) / C + 1) : 0;
+  };
+  auto row_of = [&](int first, int idx) { return 32 * (first + (idx >> 5) * C) + (idx & 31); };
+  // Tasks above block blk (L^T): 8 per column group of this CTA's own rows.
+  auto tasks_above = [&](int blk) { return blk > rank ? 64 * ((blk - 1 - rank) / C + 1) : 0; };
+  auto col_of = [&](int t) {
+    const int cg = t >> 3;
+    return 32 * (rank + (cg >> 3) * C) + 4 * (cg & 7);
+  };
+  auto load_task = [&](int r0, int m, int t, int tasks, float4 (&q)[4]) {
+    const int jg = t & 7;
+    const int i = col_of(t);
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = 4 * jg + jj;
+      q[jj] = (t < tasks && j < m) ? __ldg(reinterpret_cast<const float4*>(L + (size_t)(r0 + j) * n + i))
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  auto prefetch = [&](int s) {
+    if (s >= nb) return;
+    const int blk = TRANS ? nb - 1 - s : s;
+    const int r0 = 32 * blk, m = min(32, n - r0);
+    if (TRANS) {
+      const int tasks = tasks_above(blk);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) load_task(r0, m, tid + q * kTrsvThreads, tasks, w[q]);
+    } else {
+      int first;
+      const int rows = rows_below(blk, first);
+      const int i = row_of(first, tid);
+      if (tid < rows && i < n) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float4 t = __ldg(reinterpret_cast<const float4*>(L + (size_t)i * n + r0) + c);
+          v[4 * c] = t.x;
+          v[4 * c + 1] = t.y;
+          v[4 * c + 2] = t.z;
+          v[4 * c + 3] = t.w;
+        }
+      }
+    }
+  };
+  {
+    const int blk0 = TRANS ? nb - 1 : 0;
+    if (rank == blk0 % C && tid < 32) load_diag_block<TRANS>(L, n, 32 * blk0, min(32, n - 32 * blk0), e);
+  }
+  prefetch(0);
+  for (int s = 0; s < nb; ++s) {
+    const int blk = TRANS ? nb - 1 - s : s;
+    const int r0 = 32 * blk, m = min(32, n - r0);
+    const int owner = blk % C;
+    if (rank == owner && tid < 32) {
+      solve_diag_block<TRANS>(e, r0, m, x);
+      if (tid < m) sh.bcast[s & 1][tid] = x[r0 + tid];
+    }
+    if (C > 1)
+      umma::cluster_sync();
+    else
+      __syncthreads();
+    if (tid < 32) {
+      float val = 0.0f;
+      if (tid < m) val = (C > 1) ? ld_cluster_f32(&sh.bcast[s & 1][tid], (uint32_t)owner) : sh.bcast[s & 1][tid];
+      sh.xb[tid] = val;
+    }
+    // The next step's diagonal block (e is free again).
+    if (s + 1 < nb) {
+      const int nblk = TRANS ? blk - 1 : blk + 1;
+      if (rank == nblk % C && tid < 32) load_diag_block<TRANS>(L, n, 32 * nblk, min(32, n - 32 * nblk), e);
+    }
+    __syncthreads();
+    if (!TRANS) {
+      int first;
+      const int rows = rows_below(blk, first);
+      for (int idx = tid; idx < rows; idx += kTrsvThreads) {
+        const int i = row_of(first, idx);
+        if (i >= n) continue;
+        float a = 0.0f;
+        if (idx == tid) {
+          // The prefetched row.
+#pragma unroll
+          for (int j = 0; j < 32; ++j) a = fmaf(v[j], sh.xb[j], a);
+        } else {
+          a = row_dot32(L + (size_t)i * n + r0, sh.xb, true);
+        }
+        x[i] -= a;
+      }
+    } else {
+      const int tasks = tasks_above(blk);
+      for (int t = tid; t - tid < tasks; t += kTrsvThreads) {
+        float4 q[4];
+        const int pass = (t - tid) / kTrsvThreads;
+        if (pass == 0) {
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) q[jj] = w[0][jj];
+        } else if (pass == 1) {
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) q[jj] = w[1][jj];
+        } else {
+          load_task(r0, m, t, tasks, q);
+        }
+        const int jg = t & 7;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const float xv = sh.xb[4 * jg + jj];
+          acc.x = fmaf(q[jj].x, xv, acc.x);
+          acc.y = fmaf(q[jj].y, xv, acc.y);
+          acc.z = fmaf(q[jj].z, xv, acc.z);
+          acc.w = fmaf(q[jj].w, xv, acc.w);
+        }
+        // Sum over the eight tasks of the column group (lanes 8g .. 8g + 7).
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+          acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+          acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+          acc.z += __shfl_xor_sync(0xffffffffu, acc.z, o);
+          acc.w += __shfl_xor_sync(0xffffffffu, acc.w, o);
+        }
+        if (jg == 0 && t < tasks) {
+          const int i = col_of(t);
+          x[i] -= acc.x;
+          x[i + 1] -= acc.y;
+          x[i + 2] -= acc.z;
+          x[i + 3] -= acc.w;
+        }
+      }
+    }
+    prefetch(s + 1);
+    __syncthreads();
+  }
+}
+
 // Sum over the CTA; the result is valid in thread 0.
 __device__ __forceinline__ float cta_sum(float v, float* red) {
 #pragma unroll
@@ -210,7 +370,7 @@ __device__ __forceinline__ float cta_sum(float v, float* red) {
 // One matrix per cluster of C CTAs (launched with that cluster size).  GP:
 // b = y, xout = alpha, and loss[m] receives the log-likelihood terms.
 template <bool TRANS, bool GP>
-__global__ void __launch_bounds__(kTrsvThreads) trsv_kernel(const float* __restrict__ l, const float* b, float* xout,
+__global__ void __launch_bounds__(kTrsvThreads, 2) trsv_kernel(const float* __restrict__ l, const float* b, float* xout,
                                                             float* __restrict__ loss, int64_t batch, int n, int C) {
   extern __shared__ float xs[];
   __shared__ TrsvShared sh;
@@ -225,7 +385,10 @@ __global__ void __launch_bounds__(kTrsvThreads) trsv_kernel(const float* __restr
       if (i < n) xs[i] = b[(size_t)m * n + i];
     }
     __syncthreads();
-    cluster_trsv<TRANS>(L, n, xs, sh, C, rank);
+    if ((n & 3) == 0)
+      cluster_trsv_ahead<TRANS>(L, n, xs, sh, C, rank);
+    else
+      cluster_trsv<TRANS>(L, n, xs, sh, C, rank);
     float quad = 0.0f, logdet = 0.0f;
     for (int idx = tid; idx < 32 * nown; idx += kTrsvThreads) {
       const int i = 32 * (rank + (idx >> 5) * C) + (idx & 31);
