@@ -56,6 +56,10 @@ __device__ __forceinline__ void load_diag_block(const float* __restrict__ L, int
   }
 }
 
+__device__ __forceinline__ void st_cluster_f32(float* local, uint32_t rank, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(umma::cluster_addr(local, rank)), "f"(v) : "memory");
+}
+
 // Solves the diagonal block at rows r0 .. r0 + m - 1 in place in x (one
 // warp), with e from load_diag_block.
 template <bool TRANS>
@@ -204,7 +208,12 @@ __device__ void cluster_trsv(const float* __restrict__ L, int n, float* x, TrsvS
 // update runs, and this thread's first operands of the next update right
 // after this one, so that a step's critical path is the diagonal block's
 // shuffles, the barriers and the FMAs rather than two round trips to
-// memory.  Same barriers in the same order as cluster_trsv.  The update of
+// memory.  With C > 1 the next block's owner is idle during this step's
+// diagonal block and loads its own at the start of the step, and the owner
+// stores the 32 solved values into every CTA's shared memory ahead of the
+// cluster barrier (whose release / acquire makes them visible), so that no
+// CTA reads them remotely behind it.  Same barriers in the same order as
+// cluster_trsv.  The update of
 // L^T runs as (column group of 4, group of 4 of the block's 32 rows) tasks,
 // eight per column group in consecutive lanes, summed by shuffles.
 template <bool TRANS>
@@ -269,21 +278,29 @@ __device__ void cluster_trsv_ahead(const float* __restrict__ L, int n, float* x,
     const int blk = TRANS ? nb - 1 - s : s;
     const int r0 = 32 * blk, m = min(32, n - r0);
     const int owner = blk % C;
+    // With C > 1 the next step's owner differs from this one: its e is free.
+    if (C > 1 && s + 1 < nb) {
+      const int nblk = TRANS ? blk - 1 : blk + 1;
+      if (rank == nblk % C && tid < 32) load_diag_block<TRANS>(L, n, 32 * nblk, min(32, n - 32 * nblk), e);
+    }
     if (rank == owner && tid < 32) {
       solve_diag_block<TRANS>(e, r0, m, x);
-      if (tid < m) sh.bcast[s & 1][tid] = x[r0 + tid];
+      if (tid < m) {
+        const float val = x[r0 + tid];
+        if (C > 1) {
+          for (int q = 0; q < C; ++q) st_cluster_f32(&sh.bcast[s & 1][tid], (uint32_t)q, val);
+        } else {
+          sh.bcast[s & 1][tid] = val;
+        }
+      }
     }
     if (C > 1)
       umma::cluster_sync();
     else
       __syncthreads();
-    if (tid < 32) {
-      float val = 0.0f;
-      if (tid < m) val = (C > 1) ? ld_cluster_f32(&sh.bcast[s & 1][tid], (uint32_t)owner) : sh.bcast[s & 1][tid];
-      sh.xb[tid] = val;
-    }
-    // The next step's diagonal block (e is free again).
-    if (s + 1 < nb) {
+    if (tid < 32) sh.xb[tid] = tid < m ? sh.bcast[s & 1][tid] : 0.0f;
+    // The next step's diagonal block (C == 1: e is free again only now).
+    if (C == 1 && s + 1 < nb) {
       const int nblk = TRANS ? blk - 1 : blk + 1;
       if (rank == nblk % C && tid < 32) load_diag_block<TRANS>(L, n, 32 * nblk, min(32, n - 32 * nblk), e);
     }
