@@ -285,26 +285,26 @@ __device__ void cluster_trsv_ahead(const float* __restrict__ L, int n, float* x,
     }
     if (rank == owner && tid < 32) {
       solve_diag_block<TRANS>(e, r0, m, x);
-      if (tid < m) {
-        const float val = x[r0 + tid];
-        if (C > 1) {
-          for (int q = 0; q < C; ++q) st_cluster_f32(&sh.bcast[s & 1][tid], (uint32_t)q, val);
-        } else {
-          sh.bcast[s & 1][tid] = val;
-        }
+      // All 32 entries (zeros past a partial block), so that no value of an
+      // earlier matrix reaches the update.
+      const float val = tid < m ? x[r0 + tid] : 0.0f;
+      if (C > 1) {
+        for (int q = 0; q < C; ++q) st_cluster_f32(&sh.bcast[s & 1][tid], (uint32_t)q, val);
+      } else {
+        sh.bcast[s & 1][tid] = val;
       }
     }
+    // Barrier: the solved values are visible to every thread after it.
     if (C > 1)
       umma::cluster_sync();
     else
       __syncthreads();
-    if (tid < 32) sh.xb[tid] = tid < m ? sh.bcast[s & 1][tid] : 0.0f;
+    const float* xb = sh.bcast[s & 1];
     // The next step's diagonal block (C == 1: e is free again only now).
     if (C == 1 && s + 1 < nb) {
       const int nblk = TRANS ? blk - 1 : blk + 1;
       if (rank == nblk % C && tid < 32) load_diag_block<TRANS>(L, n, 32 * nblk, min(32, n - 32 * nblk), e);
     }
-    __syncthreads();
     if (!TRANS) {
       int first;
       const int rows = rows_below(blk, first);
@@ -315,9 +315,9 @@ __device__ void cluster_trsv_ahead(const float* __restrict__ L, int n, float* x,
         if (idx == tid) {
           // The prefetched row.
 #pragma unroll
-          for (int j = 0; j < 32; ++j) a = fmaf(v[j], sh.xb[j], a);
+          for (int j = 0; j < 32; ++j) a = fmaf(v[j], xb[j], a);
         } else {
-          a = row_dot32(L + (size_t)i * n + r0, sh.xb, true);
+          a = row_dot32(L + (size_t)i * n + r0, xb, true);
         }
         x[i] -= a;
       }
@@ -339,7 +339,7 @@ __device__ void cluster_trsv_ahead(const float* __restrict__ L, int n, float* x,
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-          const float xv = sh.xb[4 * jg + jj];
+          const float xv = xb[4 * jg + jj];
           acc.x = fmaf(q[jj].x, xv, acc.x);
           acc.y = fmaf(q[jj].y, xv, acc.y);
           acc.z = fmaf(q[jj].z, xv, acc.z);
