@@ -15,17 +15,17 @@
 // of a jitter term (Gaussian-process kernels) while the plain FP32 path
 // factors them.
 //
-// The guard therefore audits, once the tensor-mode path has factored the
-// batch, every computed pivot against
+// The guard therefore audits every computed pivot against
 //     d_j = L_jj^2  >  kGuardMargin * delta(k) * A_jj     (k = j / 64)
 // (non-finite or non-positive pivots fail too); a matrix's first failing
-// block column is its guard state.  The pivot L_jj stored by the path is
-// the one its own diagonal block produced, so the audit sees exactly what
-// a check inside the kernels would, at no cost to them.  A matrix that
-// fails is refactored from its first column in FP32 on the SIMT cores
-// (potrf_rescue.cu; the same launch does the audit and does nothing more
-// when no matrix fails).  Recomputing only from the failing column on is
-// not enough: the mixed columns before it already carry a backward error of
+// block column is its guard state.  The tensor-mode kernels record
+// (L_jj, A_jj) for each pivot next to writing L_kk, L_jj as their own
+// diagonal block produced it, and audit a matrix's record once they have
+// finished it (guard_audit_matrix), outside the diagonal engine's column
+// loop.  A matrix that fails is refactored from its first column in FP32 on
+// the SIMT cores (potrf_rescue.cu: one launch after the path, which exits
+// at once when no matrix failed).  Recomputing only from the failing column
+// on is not enough: the mixed columns before it already carry a backward error of
 // about delta * |A|, which can exceed the smallest eigenvalues of the
 // remaining Schur complement (on the Gaussian-process kernels of order 2048
 // an FP32 recompute from the failing column on still met a negative pivot,

@@ -1,4 +1,4 @@
-// Pivot audit and FP32 rescue of the pivot guard (guard.cuh).
+// FP32 rescue of the pivot guard (guard.cuh).
 //
 // The tensor-mode paths (potrf_fused.cu, potrf_fused_ws.cu, potrf_split.cu)
 // audit each matrix when they finish it (guard_audit_matrix over the
